@@ -1,0 +1,294 @@
+/*
+ * psy_b200.h - C ABI of the B200 (sm_100a) implementation of the
+ * breadth-first path-tracing hot path of the Psychopath renderer.
+ *
+ * Plain C types only: host pointers, device pointers (as void* / typed
+ * pointers into GPU memory), sizes and an opaque cudaStream_t passed as
+ * void*.  Every entry point returns an int status: PSY_OK (0) or a negative
+ * PSY_ERR_* code; psy_last_error() returns the message of the last failure
+ * on a context.  No exceptions cross this boundary.
+ *
+ * A context is used by one host thread at a time (like the reference's
+ * Tracer, one per thread: integrator/path_trace_integrator.cpp:286).
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   psy_scene_upload   Assembly::finalize -> BVH4::build + LightTree::build
+ *                      (scene/assembly.hpp:206-238, accel/bvh4.cpp:17,
+ *                      accel/light_tree.cpp:99)
+ *   psy_trace          Tracer::trace (tracer/tracer.hpp:76, tracer/tracer.cpp:38-121)
+ *   psy_trace_host     Tracer::trace with host arrays (same seam, e2e form)
+ *   psy_light_sample   LightAccel::sample / LightTree::sample
+ *                      (accel/light_accel.hpp:55, accel/light_tree.cpp:30-96)
+ *   psy_render         PathTraceIntegrator::integrate
+ *                      (integrator/integrator.hpp:32, integrator/path_trace_integrator.cpp:28-384)
+ */
+#ifndef PSY_B200_H
+#define PSY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Status codes                                                         */
+/* ------------------------------------------------------------------ */
+#define PSY_OK 0
+#define PSY_ERR_ARG (-1)            /* invalid argument / malformed scene */
+#define PSY_ERR_OOM (-2)            /* device or host allocation failed */
+#define PSY_ERR_DEVICE (-3)         /* CUDA runtime error */
+#define PSY_ERR_TIMEOUT (-4)        /* a bounded device wait gave up */
+#define PSY_ERR_STACK_OVERFLOW (-5) /* a per-ray traversal stack overflowed */
+#define PSY_ERR_NAN (-6)            /* non-finite input rejected */
+#define PSY_ERR_NO_SCENE (-7)       /* call needs a scene; none uploaded */
+
+typedef struct psy_ctx psy_ctx;
+
+/* Creates a context on CUDA device `device`. */
+int psy_ctx_create(int device, psy_ctx** out);
+void psy_ctx_destroy(psy_ctx* ctx);
+/* Message of the last failing call on ctx (never NULL). */
+const char* psy_last_error(const psy_ctx* ctx);
+/* Library version string. */
+const char* psy_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Scene description (host memory, flattened assembly tree)             */
+/* ------------------------------------------------------------------ */
+/*
+ * The flattened form of the reference's Scene / Assembly / Instance /
+ * Object / SurfaceShader graph (scene/scene.hpp:33-53,
+ * scene/assembly.hpp:26-330).  Matrices are 16 floats, row-major, in the
+ * reference's row-vector convention (v' = v * M; math/matrix.hpp:99-115).
+ * Instance transforms map the parent space into the instance's space; the
+ * camera transforms map camera space to world space.
+ */
+enum {
+	PSY_OBJ_SPHERE = 0,       /* data: n0 time samples of (cx cy cz r)            */
+	PSY_OBJ_BILINEAR = 1,     /* data: n0 time samples of 4 verts (12 floats)     */
+	PSY_OBJ_BICUBIC = 2,      /* data: n0 time samples of 16 verts (48 floats)    */
+	PSY_OBJ_SPHERE_LIGHT = 3  /* data: n0 positions (3), n1 radii, n2 colours (3) */
+};
+
+enum { PSY_INSTANCE_OBJECT = 0, PSY_INSTANCE_ASSEMBLY = 1 };
+
+enum { PSY_SHADER_LAMBERT = 0, PSY_SHADER_EMIT = 1, PSY_SHADER_GTR = 2 };
+
+typedef struct psy_object_desc {
+	uint32_t kind;         /* PSY_OBJ_* */
+	uint32_t n0, n1, n2;   /* time-sample counts (see PSY_OBJ_*) */
+	const float* data;     /* object data, layout per kind */
+} psy_object_desc;
+
+typedef struct psy_instance_desc {
+	uint32_t kind;             /* PSY_INSTANCE_* */
+	uint32_t data_index;       /* object index in the assembly, or the slot in the assembly's `children` */
+	uint32_t transform_index;  /* first transform in the assembly's transform list */
+	uint32_t transform_count;  /* motion samples; 0 = no transform */
+	int32_t shader;            /* scene shader index, -1 = none (inherit) */
+} psy_instance_desc;
+
+typedef struct psy_assembly_desc {
+	uint32_t object_count;
+	const psy_object_desc* objects;
+	uint32_t instance_count;
+	const psy_instance_desc* instances;
+	uint32_t transform_count;
+	const float* transforms;    /* transform_count * 16 */
+	uint32_t child_count;
+	const uint32_t* children;   /* scene assembly indices of the sub-assemblies */
+} psy_assembly_desc;
+
+typedef struct psy_shader_desc {
+	uint32_t kind;       /* PSY_SHADER_* */
+	float color[3];      /* RGB */
+	float roughness, tail_shape, fresnel;  /* GTR only */
+} psy_shader_desc;
+
+typedef struct psy_scene_desc {
+	uint32_t cam_transform_count;
+	const float* cam_transforms;       /* camera-to-world, count * 16 */
+	uint32_t cam_fov_count;
+	const float* cam_fovs;             /* radians (reference parser/parser.cpp:218 conversion applied) */
+	uint32_t cam_aperture_count;
+	const float* cam_aperture_radii;
+	uint32_t cam_focus_count;
+	const float* cam_focus_distances;
+	float background[3];               /* RGB */
+	float dice_rate;                   /* Config::dice_rate (config.cpp:7), 0.25 default */
+	float min_upoly_size;              /* Config::min_upoly_size (config.cpp:8), 1e-5 default */
+	uint32_t assembly_count;           /* [0] is the root assembly */
+	const psy_assembly_desc* assemblies;
+	uint32_t shader_count;
+	const psy_shader_desc* shaders;
+} psy_scene_desc;
+
+/*
+ * Builds the acceleration structures on the host exactly as
+ * Assembly::finalize does (BVH with a midpoint split, packed to BVH4; light
+ * tree) and uploads the device scene.  Replaces any previous scene.
+ */
+int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* scene);
+
+/* Summary of the uploaded scene (for tests and tooling). */
+typedef struct psy_scene_stats {
+	uint32_t assemblies, instances, objects, bvh4_nodes, light_nodes, lights;
+	uint64_t device_bytes;
+} psy_scene_stats;
+int psy_scene_stats_get(const psy_ctx* ctx, psy_scene_stats* out);
+
+/*
+ * Host-only inspection of the scene builder (no device needed): builds the
+ * scene description exactly as psy_scene_upload does and copies one
+ * assembly's BVH4 in the reference's node-record form (one record per node
+ * time sample, BVH4::Node in accel/bvh4.hpp:39-71): bounds[n*24] as BBox4
+ * SoA, child[n*3] (children 2-4, 0 = none / leaf marker), ts[n],
+ * data_index[n] (leaf instance).  Pass NULL arrays to get *count only.
+ */
+int psy_build_bvh4(const psy_scene_desc* scene, uint32_t assembly, uint64_t* count, float* bounds, uint64_t* child,
+                   uint32_t* ts, uint64_t* data_index);
+
+/*
+ * Host-only: one assembly's light tree (LightTree nodes,
+ * accel/light_tree.hpp:15-24).  meta[n*6] = is_leaf, index1, index2,
+ * instance_index, bounds count, first bounds record; energy[n];
+ * bounds[*nbounds*6] = min xyz, max xyz per time sample.  Indices are local
+ * to the assembly's tree.  Also returns the tree's light count and total
+ * energy.  Pass NULL arrays to get the counts only.
+ */
+int psy_build_light_tree(const psy_scene_desc* scene, uint32_t assembly, uint64_t* count, uint64_t* nbounds,
+                         uint64_t* meta, float* energy, float* bounds, uint64_t* light_count, float* total_energy);
+
+/* ------------------------------------------------------------------ */
+/* Ray stream tracing                                                   */
+/* ------------------------------------------------------------------ */
+/*
+ * World rays, structure of arrays (WorldRay, basics/ray.hpp:162-186).
+ * All pointers are device pointers with n elements (vec3 fields n*3).
+ */
+enum { PSY_RAY_CAMERA = 1, PSY_RAY_DIFFUSE = 2, PSY_RAY_OCCLUSION = 32 };
+
+typedef struct psy_ray_soa {
+	const float* o;       /* n*3 */
+	const float* d;       /* n*3 */
+	const float* odx;     /* n*3 origin differentials */
+	const float* ody;     /* n*3 */
+	const float* ddx;     /* n*3 direction differentials */
+	const float* ddy;     /* n*3 */
+	const float* time;    /* n */
+	const uint16_t* type; /* n, WorldRay::Type values; NULL = all closest-hit */
+} psy_ray_soa;
+
+/*
+ * Intersections, structure of arrays (Intersection, basics/intersection.hpp:22-49).
+ * Any pointer may be NULL to skip that field.  Geometry is in the hit
+ * object's space, as the reference stores it; `space` is the 4x4 transform
+ * from world space into that space at the ray's time (identity when none).
+ * closure: 0 none, 1 Lambert, 2 Emit, 3 GTR, with its RGB colour.
+ * For occlusion rays only `hit` (and `id`) are meaningful.
+ */
+typedef struct psy_hit_soa {
+	uint8_t* hit;         /* n */
+	uint64_t* id;         /* n, InstanceID bits (basics/instance_id.hpp) */
+	float* t;             /* n */
+	float* uv;            /* n*2 */
+	float* p;             /* n*3 */
+	float* n;             /* n*3 */
+	float* dpdu;          /* n*3 */
+	float* dpdv;          /* n*3 */
+	float* dndu;          /* n*3 */
+	float* dndv;          /* n*3 */
+	uint8_t* backfacing;  /* n */
+	float* light_pdf;     /* n */
+	float* offset;        /* n*3 */
+	float* space;         /* n*16 */
+	uint8_t* closure;     /* n */
+	float* closure_color; /* n*3 */
+} psy_hit_soa;
+
+/*
+ * Traces n rays (device SoA) and writes their intersections (device SoA)
+ * on `stream` (a cudaStream_t, NULL = default stream).  Asynchronous;
+ * errors from the kernel's own checks are reported by the next call that
+ * synchronises (psy_sync).
+ */
+int psy_trace(psy_ctx* ctx, const psy_ray_soa* rays, uint32_t n, const psy_hit_soa* hits, void* stream);
+
+/*
+ * The same with host arrays: copies the rays to the device, traces, copies
+ * the requested hit fields back, and synchronises.  Field layout as above,
+ * host pointers.
+ */
+int psy_trace_host(psy_ctx* ctx, const psy_ray_soa* rays, uint32_t n, const psy_hit_soa* hits);
+
+/* Waits for the context's work on `stream` and reports device-side errors. */
+int psy_sync(psy_ctx* ctx, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Light sampling                                                       */
+/* ------------------------------------------------------------------ */
+/*
+ * Batched LightTree::sample queries (LightQuery, accel/light_accel.hpp:23-42)
+ * against the root assembly, with a Lambert BSDF for the tree's estimate.
+ * Inputs (device, n or n*3): n u v, pos, nor, d, wavelength, time.
+ * Outputs (device): to_light n*3, spec n*4 (spectral sample energies),
+ * selection_pdf n, light_pdf n, id n (may be NULL).
+ */
+typedef struct psy_light_query_soa {
+	const float* n;
+	const float* u;
+	const float* v;
+	const float* pos;
+	const float* nor;
+	const float* d;
+	const float* wavelength;
+	const float* time;
+} psy_light_query_soa;
+
+typedef struct psy_light_sample_soa {
+	float* to_light;
+	float* spec;
+	float* selection_pdf;
+	float* light_pdf;
+	uint64_t* id;
+} psy_light_sample_soa;
+
+int psy_light_sample(psy_ctx* ctx, const psy_light_query_soa* q, uint32_t n, const psy_light_sample_soa* out,
+                     void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Rendering                                                            */
+/* ------------------------------------------------------------------ */
+typedef struct psy_render_desc {
+	uint32_t width, height;   /* image resolution */
+	uint32_t spp;             /* samples per pixel */
+	uint32_t seed;            /* sampler seed (RenderSettings Seed) */
+	uint32_t path_length;     /* max path segments (PathTraceIntegrator::path_length, default 4) */
+	uint32_t stream_paths;    /* paths in flight per wave, 0 = automatic */
+	uint32_t block_size;      /* threads per block for the wavefront kernels, 0 = automatic */
+} psy_render_desc;
+
+typedef struct psy_render_stats {
+	uint64_t paths;           /* width*height*spp */
+	uint64_t rays;            /* rays traced (Global::Stats::rays_shot equivalent) */
+	uint32_t launches;        /* kernels launched */
+	uint32_t waves;
+} psy_render_stats;
+
+/*
+ * Renders the uploaded scene.  xyz (device, width*height*3) receives the
+ * per-pixel XYZ sums of the samples, each scaled by XYZ_NORM_FAC exactly as
+ * Film::add_sample receives them (path_trace_integrator.cpp:357-359);
+ * counts (device, width*height, may be NULL) the accepted sample counts.
+ * Both are accumulated into (not cleared).  Stream-ordered on `stream`.
+ */
+int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* counts, psy_render_stats* stats,
+               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSY_B200_H */

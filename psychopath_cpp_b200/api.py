@@ -1,0 +1,281 @@
+"""Python host mirror of the reference's hot-path interfaces, over the C ABI.
+
+    Context            one psy_ctx (a CUDA device + uploaded scene)
+    Tracer             Tracer::trace (reference tracer/tracer.hpp:76)
+    LightTree          LightTree::sample (reference accel/light_tree.cpp:30)
+    PathTraceIntegrator PathTraceIntegrator::integrate
+                       (reference integrator/path_trace_integrator.hpp:103-126)
+
+Scenes are the psychopath_cpp_b200.scene model (or .psy files through
+scene.read_psy); ``flatten`` turns one into the C ABI's psy_scene_desc.
+Every call goes through libpsy_b200.so; a missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from . import _abi
+from .scene import (Assembly, BicubicPatch, BilinearPatch, Scene, Sphere, SphereLight, SurfaceShader)
+
+F32 = np.float32
+
+HIT_FIELDS = {  # name -> (dtype, per-ray width)
+    "hit": (np.uint8, 1), "id": (np.uint64, 1), "t": (np.float32, 1), "uv": (np.float32, 2),
+    "p": (np.float32, 3), "n": (np.float32, 3), "dpdu": (np.float32, 3), "dpdv": (np.float32, 3),
+    "dndu": (np.float32, 3), "dndv": (np.float32, 3), "backfacing": (np.uint8, 1),
+    "light_pdf": (np.float32, 1), "offset": (np.float32, 3), "space": (np.float32, 16),
+    "closure": (np.uint8, 1), "closure_color": (np.float32, 3),
+}
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+# --------------------------------------------------------------------------
+# Scene flattening
+# --------------------------------------------------------------------------
+
+def flatten(scene: Scene):
+    """Returns (SceneDesc, keepalive) for psy_scene_upload."""
+    keep: List = []
+    asm_order: List[Assembly] = []
+
+    def collect(a: Assembly):
+        asm_order.append(a)
+        for sub in a.assemblies.values():
+            collect(sub)
+
+    collect(scene.root)
+    asm_index = {id(a): i for i, a in enumerate(asm_order)}
+    shader_list: List[SurfaceShader] = []
+    shader_index: Dict[int, int] = {}
+
+    def shader_id(sh: Optional[SurfaceShader]) -> int:
+        if sh is None:
+            return -1
+        if id(sh) not in shader_index:
+            shader_index[id(sh)] = len(shader_list)
+            shader_list.append(sh)
+        return shader_index[id(sh)]
+
+    asm_descs = (_abi.AssemblyDesc * len(asm_order))()
+    for ai, a in enumerate(asm_order):
+        obj_names = list(a.objects.keys())
+        sub_names = list(a.assemblies.keys())
+        obj_pos = {name: i for i, name in enumerate(obj_names)}
+        sub_pos = {name: i for i, name in enumerate(sub_names)}
+        objs = (_abi.ObjectDesc * max(1, len(obj_names)))()
+        for oi, name in enumerate(obj_names):
+            ob = a.objects[name]
+            if isinstance(ob, Sphere):
+                data = np.concatenate([ob.location, [ob.radius]]).astype(F32)
+                kind, n0, n1, n2 = _abi.PSY_OBJ_SPHERE, 1, 0, 0
+            elif isinstance(ob, BilinearPatch):
+                data = ob.verts.reshape(-1).astype(F32)
+                kind, n0, n1, n2 = _abi.PSY_OBJ_BILINEAR, ob.verts.shape[0], 0, 0
+            elif isinstance(ob, BicubicPatch):
+                data = ob.verts.reshape(-1).astype(F32)
+                kind, n0, n1, n2 = _abi.PSY_OBJ_BICUBIC, ob.verts.shape[0], 0, 0
+            elif isinstance(ob, SphereLight):
+                data = np.concatenate([ob.locations.ravel(), ob.radii.ravel(), ob.colors.ravel()]).astype(F32)
+                kind, n0, n1, n2 = (_abi.PSY_OBJ_SPHERE_LIGHT, ob.locations.shape[0], ob.radii.shape[0],
+                                    ob.colors.shape[0])
+            else:
+                raise TypeError("unsupported object %r" % type(ob))
+            data = np.ascontiguousarray(data)
+            keep.append(data)
+            objs[oi] = _abi.ObjectDesc(kind, n0, n1, n2, data.ctypes.data_as(_abi.fp))
+        xforms: List[np.ndarray] = []
+        insts = (_abi.InstanceDesc * max(1, len(a.instances)))()
+        for ii, inst in enumerate(a.instances):
+            if inst.data in obj_pos:
+                kind, didx = _abi.PSY_INSTANCE_OBJECT, obj_pos[inst.data]
+            elif inst.data in sub_pos:
+                kind, didx = _abi.PSY_INSTANCE_ASSEMBLY, sub_pos[inst.data]
+            else:
+                raise KeyError("instance of unknown data %r" % inst.data)
+            sh = a.find_shader(inst.shader) if inst.shader is not None else None
+            insts[ii] = _abi.InstanceDesc(kind, didx, len(xforms), len(inst.transforms), shader_id(sh))
+            xforms.extend(inst.transforms)
+        xf = np.ascontiguousarray(np.array(xforms, dtype=F32).reshape(-1)) if xforms else np.zeros(16, F32)
+        children = np.array([asm_index[id(a.assemblies[n])] for n in sub_names] or [0], dtype=np.uint32)
+        keep += [objs, insts, xf, children]
+        asm_descs[ai] = _abi.AssemblyDesc(len(obj_names), objs, len(a.instances), insts, len(xforms),
+                                          xf.ctypes.data_as(_abi.fp), len(sub_names),
+                                          children.ctypes.data_as(_abi.u32p))
+    shaders = (_abi.ShaderDesc * max(1, len(shader_list)))()
+    kinds = {"Lambert": _abi.PSY_SHADER_LAMBERT, "Emit": _abi.PSY_SHADER_EMIT, "GTR": _abi.PSY_SHADER_GTR}
+    for si, sh in enumerate(shader_list):
+        shaders[si] = _abi.ShaderDesc(kinds[sh.kind], (C.c_float * 3)(*[float(c) for c in sh.color]),
+                                      float(sh.roughness), float(sh.tail_shape), float(sh.fresnel))
+    cam = scene.camera
+    cx = np.ascontiguousarray(np.array(cam.transforms, dtype=F32).reshape(-1))
+    fovs = np.ascontiguousarray(cam.fovs_radians())
+    aps = np.ascontiguousarray(np.array(cam.aperture_radii or [0.0], dtype=F32))
+    foc = np.ascontiguousarray(np.array(cam.focus_distances or [1.0], dtype=F32))
+    keep += [asm_descs, shaders, cx, fovs, aps, foc]
+    d = _abi.SceneDesc()
+    d.cam_transform_count = len(cam.transforms)
+    d.cam_transforms = cx.ctypes.data_as(_abi.fp)
+    d.cam_fov_count = len(fovs)
+    d.cam_fovs = fovs.ctypes.data_as(_abi.fp)
+    d.cam_aperture_count = len(cam.aperture_radii)
+    d.cam_aperture_radii = aps.ctypes.data_as(_abi.fp)
+    d.cam_focus_count = len(cam.focus_distances)
+    d.cam_focus_distances = foc.ctypes.data_as(_abi.fp)
+    for k in range(3):
+        d.background[k] = float(scene.background[k])
+    d.dice_rate = float(F32(scene.dicing_rate if scene.dicing_rate is not None else 0.25))
+    d.min_upoly_size = float(F32(0.00001))
+    d.assembly_count = len(asm_order)
+    d.assemblies = asm_descs
+    d.shader_count = len(shader_list)
+    d.shaders = shaders
+    return d, keep
+
+
+# --------------------------------------------------------------------------
+# Context and reference-named wrappers
+# --------------------------------------------------------------------------
+
+class Context:
+    """A psy_ctx on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.L = _abi.load()
+        h = C.c_void_p()
+        rc = self.L.psy_ctx_create(device, C.byref(h))
+        if rc != 0:
+            raise _abi.PsyError(rc, "psy_ctx_create(%d) failed" % device)
+        self.h = h
+        self.device = device
+        self.scene: Optional[Scene] = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.psy_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc: int):
+        if rc != 0:
+            raise _abi.PsyError(rc, self.L.psy_last_error(self.h).decode())
+
+    def upload(self, scene: Scene) -> None:
+        desc, keep = flatten(scene)
+        self.check(self.L.psy_scene_upload(self.h, C.byref(desc)))
+        del keep
+        self.scene = scene
+
+    def stats(self) -> dict:
+        s = _abi.SceneStats()
+        self.check(self.L.psy_scene_stats_get(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in _abi.SceneStats._fields_}
+
+    def sync(self, stream=None):
+        self.check(self.L.psy_sync(self.h, stream))
+
+
+def _check(L, rc: int, what: str):
+    if rc != 0:
+        raise _abi.PsyError(rc, what)
+
+
+def build_bvh4_records(scene: Scene, assembly: int = 0) -> dict:
+    """Host-only: the BVH4 node records the builder produces for one
+    assembly, in the reference's BVH4::Node form (psy_build_bvh4)."""
+    L = _abi.load()
+    desc, keep = flatten(scene)
+    n = C.c_uint64()
+    _check(L, L.psy_build_bvh4(C.byref(desc), assembly, C.byref(n), None, None, None, None), "psy_build_bvh4")
+    k = n.value
+    b = np.zeros((k, 24), F32)
+    ch = np.zeros((k, 3), np.uint64)
+    ts = np.zeros(k, np.uint32)
+    di = np.zeros(k, np.uint64)
+    _check(L, L.psy_build_bvh4(C.byref(desc), assembly, C.byref(n), b.ctypes.data_as(_abi.fp),
+                               ch.ctypes.data_as(_abi.u64p), ts.ctypes.data_as(_abi.u32p),
+                               di.ctypes.data_as(_abi.u64p)), "psy_build_bvh4")
+    del keep
+    return {"bounds": b, "child": ch, "ts": ts, "data_index": di}
+
+
+def build_light_tree(scene: Scene, assembly: int = 0) -> dict:
+    """Host-only: the light tree the builder produces for one assembly
+    (psy_build_light_tree), in the reference's LightTree node form."""
+    L = _abi.load()
+    desc, keep = flatten(scene)
+    n, nb, lc = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    te = C.c_float()
+    _check(L, L.psy_build_light_tree(C.byref(desc), assembly, C.byref(n), C.byref(nb), None, None, None,
+                                     C.byref(lc), C.byref(te)), "psy_build_light_tree")
+    meta = np.zeros((n.value, 6), np.uint64)
+    en = np.zeros(n.value, F32)
+    bb = np.zeros((max(nb.value, 1), 6), F32)
+    _check(L, L.psy_build_light_tree(C.byref(desc), assembly, C.byref(n), C.byref(nb),
+                                     meta.ctypes.data_as(_abi.u64p), en.ctypes.data_as(_abi.fp),
+                                     bb.ctypes.data_as(_abi.fp), C.byref(lc), C.byref(te)), "psy_build_light_tree")
+    del keep
+    return {"meta": meta, "energy": en, "bounds": bb[:nb.value], "light_count": lc.value,
+            "total_energy": te.value}
+
+
+def _ray_soa_host(rays: dict) -> Tuple[_abi.RaySoA, list]:
+    keep = []
+
+    def a(name, dtype, shape):
+        arr = np.ascontiguousarray(np.asarray(rays[name], dtype=dtype).reshape(shape))
+        keep.append(arr)
+        return arr.ctypes.data_as(C.c_void_p)
+
+    n = len(rays["time"])
+    r = _abi.RaySoA(a("o", F32, (n, 3)), a("d", F32, (n, 3)), a("odx", F32, (n, 3)), a("ody", F32, (n, 3)),
+                    a("ddx", F32, (n, 3)), a("ddy", F32, (n, 3)), a("time", F32, (n,)),
+                    a("type", np.uint16, (n,)) if "type" in rays else None)
+    return r, keep
+
+
+class Tracer:
+    """Tracer::trace over a ray stream (reference tracer/tracer.cpp:38-121)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def trace(self, rays: dict, fields=("hit", "id", "t", "uv")) -> Dict[str, np.ndarray]:
+        """Host-array form (psy_trace_host): returns the requested
+        Intersection fields as numpy arrays."""
+        n = len(rays["time"])
+        rs, keep = _ray_soa_host(rays)
+        out = {}
+        hs = _abi.HitSoA()
+        for f in fields:
+            dt, w = HIT_FIELDS[f]
+            arr = np.zeros((n, w) if w > 1 else (n,), dt)
+            out[f] = arr
+            setattr(hs, f, arr.ctypes.data_as(C.c_void_p))
+        self.ctx.check(self.ctx.L.psy_trace_host(self.ctx.h, C.byref(rs), n, C.byref(hs)))
+        return out
+
+    def trace_device(self, rays: dict, hits: dict, stream=None) -> None:
+        """Device form (psy_trace): `rays` and `hits` map field names to
+        CUDA tensors (anything with .data_ptr()); stream-ordered."""
+        n = int(rays["time"].shape[0])
+
+        def p(t):
+            return None if t is None else C.c_void_p(t.data_ptr())
+
+        rs = _abi.RaySoA(p(rays["o"]), p(rays["d"]), p(rays["odx"]), p(rays["ody"]), p(rays["ddx"]),
+                         p(rays["ddy"]), p(rays["time"]), p(rays.get("type")))
+        hs = _abi.HitSoA()
+        for f, t in hits.items():
+            setattr(hs, f, p(t))
+        self.ctx.check(self.ctx.L.psy_trace(self.ctx.h, C.byref(rs), n, C.byref(hs), stream))

@@ -1,0 +1,50 @@
+/*
+ * The context object behind the opaque psy_ctx handle.
+ */
+#ifndef PSY_CTX_H
+#define PSY_CTX_H
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "psy_scene.h"
+#include "scene_build.h"
+
+#define PSY_MAX_LEVELS_HOST 8
+
+struct psy_ctx {
+	struct Scratch {
+		void* ptr = nullptr;
+		size_t bytes = 0;
+	};
+
+	int device = 0;
+	std::string last_error;
+	bool has_scene = false;
+	std::unique_ptr<psy::BuiltScene> host;
+	std::vector<void*> scene_allocs;
+	psy::DevScene dev{};
+	size_t device_bytes = 0;
+	unsigned* d_status = nullptr;
+	unsigned* h_status = nullptr;
+	std::map<std::string, Scratch> scratch;
+	cudaStream_t stream_ = nullptr;
+
+	~psy_ctx();
+	void free_scene();
+	int upload(const void* src, size_t bytes, void** dst);
+	// A named device buffer of at least `bytes`, reused between calls.
+	void* scratch_buffer(const char* name, size_t bytes, int* rc);
+	// Synchronises `stream`, reads and clears the device status word.
+	int check_status(cudaStream_t stream);
+	cudaStream_t host_stream() { return stream_; }
+};
+
+int ctx_fail(psy_ctx* ctx, int code, const char* fmt, ...);
+int ctx_cuda(psy_ctx* ctx, cudaError_t e, const char* what);
+
+#endif

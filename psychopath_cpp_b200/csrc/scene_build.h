@@ -1,0 +1,51 @@
+/*
+ * Host-side scene preparation: the equivalent of Assembly::finalize
+ * (reference scene/assembly.hpp:206-238) for a flattened scene description.
+ */
+#ifndef PSY_SCENE_BUILD_H
+#define PSY_SCENE_BUILD_H
+
+#include <string>
+#include <vector>
+
+#include "../../include/psy_b200.h"
+#include "psy_scene.h"
+
+namespace psy {
+
+// BVH4 node records in the reference's own form (BVH4::Node, accel/bvh4.hpp:39-71),
+// kept for inspection and parity tests of the builder.
+struct RefBVH4 {
+	std::vector<float> bounds;        // 24 per record
+	std::vector<uint64_t> child;      // 3 per record
+	std::vector<uint32_t> ts;
+	std::vector<uint64_t> data_index;
+};
+
+struct BuiltScene {
+	std::vector<DevAssembly> assemblies;
+	std::vector<DevInstance> instances;
+	std::vector<DevObject> objects;
+	std::vector<DevNode> nodes;
+	std::vector<float> node_extra;
+	std::vector<float> xforms;
+	std::vector<float> fpool;
+	std::vector<DevLightNode> light_nodes;
+	std::vector<float> light_extra;
+	std::vector<DevShader> shaders;
+	std::vector<float> cam_xforms, cam_tfovs, cam_apertures, cam_focus;
+	float background[3] = {0, 0, 0};
+	float dice_rate = 0.25f;
+	float min_upoly_size = 0.00001f;
+	int max_depth = 1;
+	uint32_t total_lights = 0;
+	std::vector<RefBVH4> ref_bvh4;    // per assembly
+};
+
+// Validates the description and builds every assembly (children first).
+// Returns PSY_OK or PSY_ERR_ARG with *err set.
+int build_scene(const psy_scene_desc* desc, BuiltScene* out, std::string* err);
+
+}  // namespace psy
+
+#endif

@@ -1,0 +1,654 @@
+/*
+ * Device-side ray traversal of the uploaded scene: one ray per thread.
+ *
+ * The reference traces ray *streams* breadth-first (accel/bvh4.cpp:163-236,
+ * object/patch_utils.hpp:18-200); every per-ray decision there depends only
+ * on that ray's own state, so a depth-first per-ray walk that keeps the
+ * reference's tests and its max_t updates returns the same closest hit.  The
+ * one order-dependent case, two candidates at exactly the same t, resolves
+ * to whichever is found first; child boxes are visited nearest-first here.
+ *
+ * Per-ray state: the ray in the current instance space, a node stack,
+ * a level stack for nested assemblies (element id prefix, inherited shader,
+ * merged motion transforms, as the reference's xform_stack /
+ * surface_shader_stack / element_id, tracer/tracer.cpp:125-219), and a
+ * patch-split stack for the bisection of a patch (SPLIT_STACK_SIZE 64,
+ * object/patch_utils.hpp:16).
+ */
+#ifndef PSY_TRACE_DEVICE_CUH
+#define PSY_TRACE_DEVICE_CUH
+
+#include "psy_math.h"
+#include "psy_scene.h"
+
+namespace psy {
+
+#define PSY_NODE_STACK 64
+#define PSY_MAX_LEVELS 8
+#define PSY_MAX_MOTION 4
+#define PSY_SPLIT_STACK 64
+
+
+struct WorldRayD {
+	V3 o, d, odx, ody, ddx, ddy;
+	float time;
+	bool occl;
+};
+
+// Ray in the current instance space (Ray, basics/ray.hpp:24-37).
+struct LocalRay {
+	V3 o, d, dinv;
+	RayWidth w;
+};
+
+__device__ __forceinline__ M44 load_m44_dev(const float* p) {
+	M44 m;
+	const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+	for (int r = 0; r < 4; ++r) {
+		const float4 v = __ldg(q + r);
+		m.m[r][0] = v.x;
+		m.m[r][1] = v.y;
+		m.m[r][2] = v.z;
+		m.m[r][3] = v.w;
+	}
+	return m;
+}
+
+// WorldRay::update_ray (basics/ray.hpp:207-305): with and without transform.
+__device__ __forceinline__ LocalRay make_local(const WorldRayD& wr) {
+	LocalRay r;
+	r.o = wr.o;
+	r.d = wr.d;
+	r.w = ray_width_params(r.o, r.d, wr.odx, wr.ody, wr.ddx, wr.ddy);
+	r.dinv = recip3(r.d);
+	return r;
+}
+
+__device__ __forceinline__ LocalRay make_local_x(const WorldRayD& wr, const M44& t) {
+	LocalRay r;
+	r.o = pos_to(t, wr.o);
+	r.d = dir_to(t, wr.d);
+	r.w = ray_width_params(r.o, r.d, dir_to(t, wr.odx), dir_to(t, wr.ody), dir_to(t, wr.ddx), dir_to(t, wr.ddy));
+	r.dinv = recip3(r.d);
+	return r;
+}
+
+// Merged motion-transform sequence of a level (the reference's xform_stack frame).
+struct Frame {
+	int count;  // 0 = no transform (identity)
+	M44 m[PSY_MAX_MOTION];
+};
+
+__device__ __forceinline__ M44 frame_at_index_lerp(const Frame& f, float alpha) {
+	const SeqPos sp = seq_pos(alpha, f.count);
+	if (sp.single) return f.m[sp.i0];
+	return m44_lerp(sp.nalpha, f.m[sp.i0], f.m[sp.i0 + 1]);
+}
+
+__device__ __forceinline__ M44 seq_lerp_global(const float* xs, int count, float alpha) {
+	const SeqPos sp = seq_pos(alpha, count);
+	if (sp.single) return load_m44_dev(xs + 16 * sp.i0);
+	return m44_lerp(sp.nalpha, load_m44_dev(xs + 16 * sp.i0), load_m44_dev(xs + 16 * (sp.i0 + 1)));
+}
+
+// merge() of transform sequences (math/transform.hpp:241-272): parent `a`
+// with instance transforms `b` (global, count nb), written into `dst`.
+// Returns false if the result needs more than PSY_MAX_MOTION samples.
+__device__ __forceinline__ bool frame_merge(const Frame& a, const float* b, int nb, Frame* dst) {
+	const int na = a.count;
+	if (na > PSY_MAX_MOTION || nb > PSY_MAX_MOTION) return false;
+	if (na == nb) {
+		for (int i = 0; i < na; ++i) dst->m[i] = m44_mul(a.m[i], load_m44_dev(b + 16 * i));
+		dst->count = na;
+	} else if (na > nb) {
+		if (nb == 0) {
+			for (int i = 0; i < na; ++i) dst->m[i] = a.m[i];
+		} else {
+			const float inv_s = 1.0f / (float)(na - 1);
+			for (int i = 0; i < na; ++i) dst->m[i] = m44_mul(a.m[i], seq_lerp_global(b, nb, (float)i * inv_s));
+		}
+		dst->count = na;
+	} else {
+		if (na == 0) {
+			for (int i = 0; i < nb; ++i) dst->m[i] = load_m44_dev(b + 16 * i);
+		} else {
+			const float inv_s = 1.0f / (float)(nb - 1);
+			// The reference multiplies instance * lerped-parent in this branch.
+			for (int i = 0; i < nb; ++i) dst->m[i] = m44_mul(load_m44_dev(b + 16 * i), frame_at_index_lerp(a, (float)i * inv_s));
+		}
+		dst->count = nb;
+	}
+	return true;
+}
+
+// ---------------------------------------------------------------------
+// Sphere / sphere light intersection (object/sphere.cpp:67-189,
+// lights/sphere_light.hpp:159-246): returns the hit t or -1.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ float sphere_t(V3 ro, V3 rd, V3 cent, float radi, float max_t) {
+	const V3 o = ro - cent;
+	const V3 d = rd;
+	const float a = length2(d);
+	const float b = 2.0f * dot(d, o);
+	const float c = length2(o) - radi * radi;
+	float disc = b * b - 4.0f * a * c;
+	if (disc < 0.0f) return -1.0f;
+	disc = sqrtf(disc);
+	float q;
+	if (b < 0.0f) q = -0.5f * (b - disc);
+	else q = -0.5f * (b + disc);
+	float t0 = q / a;
+	float t1;
+	if (q != 0.0f) t1 = c / q;
+	else t1 = max_t;
+	if (t0 > t1) {
+		const float tmp = t1;
+		t1 = t0;
+		t0 = tmp;
+	}
+	if (t0 >= max_t || t1 < 0.0001f) return -1.0f;
+	if (t0 >= 0.0001f) return t0;
+	if (t1 < max_t) return t1;
+	return -1.0f;
+}
+
+__device__ __forceinline__ void sphere_at(const DevScene& sc, const DevObject& ob, float time, V3* cent, float* radi) {
+	const float* p = sc.fpool + ob.data;
+	const SeqPos sp = seq_pos(time, ob.n0);
+	if (sp.single) {
+		*cent = V3(p[sp.i0 * 4], p[sp.i0 * 4 + 1], p[sp.i0 * 4 + 2]);
+		*radi = p[sp.i0 * 4 + 3];
+	} else {
+		const float* a = p + sp.i0 * 4;
+		const float* b = a + 4;
+		*cent = lerp3(sp.nalpha, V3(a[0], a[1], a[2]), V3(b[0], b[1], b[2]));
+		*radi = lerp1(sp.nalpha, a[3], b[3]);
+	}
+}
+
+__device__ __forceinline__ void light_at(const DevScene& sc, const DevObject& ob, float time, V3* pos, float* radi,
+                                         float col[3]) {
+	const float* p = sc.fpool + ob.data;
+	{
+		const SeqPos sp = seq_pos(time, ob.n0);
+		const float* a = p + sp.i0 * 3;
+		if (sp.single) *pos = V3(a[0], a[1], a[2]);
+		else *pos = lerp3(sp.nalpha, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]));
+	}
+	const float* rp = p + ob.n0 * 3;
+	{
+		const SeqPos sp = seq_pos(time, ob.n1);
+		if (sp.single) *radi = rp[sp.i0];
+		else *radi = lerp1(sp.nalpha, rp[sp.i0], rp[sp.i0 + 1]);
+	}
+	const float* cp = rp + ob.n1;
+	{
+		const SeqPos sp = seq_pos(time, ob.n2);
+		const float* a = cp + sp.i0 * 3;
+		if (sp.single) {
+			col[0] = a[0]; col[1] = a[1]; col[2] = a[2];
+		} else {
+			const float ia = one_minus(sp.nalpha);
+			for (int k = 0; k < 3; ++k) col[k] = (a[k] * ia) + (a[3 + k] * sp.nalpha);
+		}
+	}
+}
+
+// ---------------------------------------------------------------------
+// Patches (object/bilinear.hpp, object/bicubic.hpp)
+// ---------------------------------------------------------------------
+template <int NV>
+struct Patch {
+	V3 p[NV];
+};
+
+template <int NV>
+__device__ __forceinline__ Box patch_bound(const Patch<NV>& q) {
+	Box b;
+	b.lo = q.p[0];
+	b.hi = q.p[0];
+#pragma unroll
+	for (int i = 1; i < NV; ++i) {
+		b.lo = vmin3(b.lo, q.p[i]);
+		b.hi = vmax3(b.hi, q.p[i]);
+	}
+	return b;
+}
+
+__device__ __forceinline__ float patch_ulen(const Patch<4>& q) { return longest_axis(q.p[0] - q.p[1]); }
+__device__ __forceinline__ float patch_vlen(const Patch<4>& q) { return longest_axis(q.p[0] - q.p[2]); }
+__device__ __forceinline__ float patch_ulen(const Patch<16>& q) { return longest_axis(q.p[0] - q.p[3]); }
+__device__ __forceinline__ float patch_vlen(const Patch<16>& q) { return longest_axis(q.p[0] - q.p[12]); }
+
+// Bilinear::split_u / split_v: p1 = first half (written in place), p2 = second half.
+__device__ __forceinline__ void patch_split_u(Patch<4>& p, Patch<4>* p2) {
+	const V3 m01 = (p.p[0] + p.p[1]) * 0.5f;
+	const V3 m23 = (p.p[2] + p.p[3]) * 0.5f;
+	p2->p[0] = m01;
+	p2->p[1] = p.p[1];
+	p2->p[2] = m23;
+	p2->p[3] = p.p[3];
+	p.p[1] = m01;
+	p.p[3] = m23;
+}
+__device__ __forceinline__ void patch_split_v(Patch<4>& p, Patch<4>* p2) {
+	const V3 m02 = (p.p[0] + p.p[2]) * 0.5f;
+	const V3 m13 = (p.p[1] + p.p[3]) * 0.5f;
+	p2->p[0] = m02;
+	p2->p[1] = m13;
+	p2->p[2] = p.p[2];
+	p2->p[3] = p.p[3];
+	p.p[2] = m02;
+	p.p[3] = m13;
+}
+
+// Bicubic::split_u / split_v (de Casteljau at 0.5 per row / column).
+__device__ __forceinline__ void patch_split_u(Patch<16>& p, Patch<16>* p2) {
+#pragma unroll
+	for (int r = 0; r < 4; ++r) {
+		const int rr = r * 4;
+		const V3 tmp = (p.p[rr + 1] + p.p[rr + 2]) * 0.5f;
+		const V3 q3 = p.p[rr + 3];
+		const V3 q2 = (p.p[rr + 3] + p.p[rr + 2]) * 0.5f;
+		const V3 q1 = (tmp + q2) * 0.5f;
+		const V3 a0 = p.p[rr + 0];
+		const V3 a1 = (p.p[rr + 0] + p.p[rr + 1]) * 0.5f;
+		const V3 a2 = (tmp + a1) * 0.5f;
+		const V3 a3 = (a2 + q1) * 0.5f;
+		p2->p[rr + 3] = q3;
+		p2->p[rr + 2] = q2;
+		p2->p[rr + 1] = q1;
+		p2->p[rr + 0] = a3;
+		p.p[rr + 0] = a0;
+		p.p[rr + 1] = a1;
+		p.p[rr + 2] = a2;
+		p.p[rr + 3] = a3;
+	}
+}
+__device__ __forceinline__ void patch_split_v(Patch<16>& p, Patch<16>* p2) {
+#pragma unroll
+	for (int c = 0; c < 4; ++c) {
+		const V3 tmp = (p.p[c + 4] + p.p[c + 8]) * 0.5f;
+		const V3 q3 = p.p[c + 12];
+		const V3 q2 = (p.p[c + 12] + p.p[c + 8]) * 0.5f;
+		const V3 q1 = (tmp + q2) * 0.5f;
+		const V3 a0 = p.p[c + 0];
+		const V3 a1 = (p.p[c + 0] + p.p[c + 4]) * 0.5f;
+		const V3 a2 = (tmp + a1) * 0.5f;
+		const V3 a3 = (a2 + q1) * 0.5f;
+		p2->p[c + 12] = q3;
+		p2->p[c + 8] = q2;
+		p2->p[c + 4] = q1;
+		p2->p[c + 0] = a3;
+		p.p[c + 0] = a0;
+		p.p[c + 4] = a1;
+		p.p[c + 8] = a2;
+		p.p[c + 12] = a3;
+	}
+}
+
+template <int NV>
+__device__ __forceinline__ void patch_load(const float* src, Patch<NV>* q) {
+#pragma unroll
+	for (int i = 0; i < NV; ++i) q->p[i] = V3(__ldg(src + i * 3), __ldg(src + i * 3 + 1), __ldg(src + i * 3 + 2));
+}
+
+// Result of a patch leaf hit, consumed by the shading epilogue.
+struct PatchHit {
+	float t, u, v, max_dim;
+};
+
+// Per-ray bisection of one patch with TSC time samples (TSC = 1 or 2):
+// intersect_rays_with_patch for a single ray (object/patch_utils.hpp:18-200).
+// The second half of every split is visited first, as in the reference.
+// Returns true when a new closest hit was recorded (or, for occlusion rays,
+// when any leaf was hit).
+template <int NV, int TSC>
+__device__ bool patch_intersect(const float* verts, float time, const LocalRay& r, float* max_t, bool occl,
+                                float dice_rate, float min_upoly, PatchHit* hit) {
+	struct Entry {
+		Patch<NV> q[TSC];
+		float u0, u1, v0, v1;
+	};
+	Entry stack[PSY_SPLIT_STACK];
+	int sp = 0;
+	Entry cur;
+#pragma unroll
+	for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur.q[k]);
+	cur.u0 = 0.0f; cur.u1 = 1.0f; cur.v0 = 0.0f; cur.v1 = 1.0f;
+	int t_index = 0;
+	float t_nalpha = 0.0f;
+	if (TSC > 1) {
+		const float t_time = time * (float)(TSC - 1);
+		t_index = (int)t_time;
+		t_nalpha = t_time - (float)t_index;
+		// time == 1.0 would index past the last sample (undefined in the
+		// reference); clamp to the last segment
+		if (t_index > TSC - 2) t_index = TSC - 2;
+	}
+	bool found = false;
+	int depth = 0;           // stack_i of the reference for `cur`
+	int depth_stack[PSY_SPLIT_STACK];
+	while (true) {
+		Box bb[TSC];
+		float max_dim = 0.0f;
+#pragma unroll
+		for (int k = 0; k < TSC; ++k) {
+			bb[k] = patch_bound<NV>(cur.q[k]);
+			const float ld = longest_axis(bb[k].hi - bb[k].lo);
+			max_dim = (k == 0) ? ld : smax(max_dim, ld);
+		}
+		float h0, h1;
+		bool h;
+		if (TSC == 1) h = box_hit(bb[0], r.o, r.dinv, *max_t, &h0, &h1);
+		else h = box_hit(box_lerp(t_nalpha, bb[t_index], bb[t_index + 1]), r.o, r.dinv, *max_t, &h0, &h1);
+		bool descend = false;
+		if (h) {
+			const float width = smax(ray_min_width(r.w, h0, h1) * dice_rate, min_upoly);
+			if (max_dim <= width || depth == PSY_SPLIT_STACK - 1) {
+				const float tt = (h0 + h1) * 0.5f;
+				if (tt > 0.0f && tt < *max_t) {
+					found = true;
+					if (occl) return true;
+					*max_t = tt;
+					hit->t = tt;
+					hit->u = (cur.u0 + cur.u1) * 0.5f;
+					hit->v = (cur.v0 + cur.v1) * 0.5f;
+					hit->max_dim = max_dim;
+				}
+			} else {
+				descend = true;
+			}
+		}
+		if (descend) {
+			// split: `cur` keeps the first half (pushed), the second half is next
+			Entry second;
+			const float ul = patch_ulen(cur.q[0]);
+			const float vl = patch_vlen(cur.q[0]);
+			if (ul > vl) {
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) patch_split_u(cur.q[k], &second.q[k]);
+				const float um = (cur.u0 + cur.u1) * 0.5f;
+				second.u0 = um; second.u1 = cur.u1; second.v0 = cur.v0; second.v1 = cur.v1;
+				cur.u1 = um;
+			} else {
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) patch_split_v(cur.q[k], &second.q[k]);
+				const float vm = (cur.v0 + cur.v1) * 0.5f;
+				second.u0 = cur.u0; second.u1 = cur.u1; second.v0 = vm; second.v1 = cur.v1;
+				cur.v1 = vm;
+			}
+			stack[sp] = cur;
+			depth_stack[sp] = depth;
+			++sp;
+			cur = second;
+			depth = depth + 1;
+		} else {
+			if (sp == 0) break;
+			--sp;
+			cur = stack[sp];
+			depth = depth_stack[sp];
+		}
+	}
+	return found;
+}
+
+// ---------------------------------------------------------------------
+// Whole-scene traversal
+// ---------------------------------------------------------------------
+struct HitRec {
+	float t;
+	float u, v, max_dim;
+	int obj;          // global object index, -1 = miss
+	int kind;
+	int shader;       // innermost bound shader, -1 = none
+	uint64_t id;
+	int depth;        // number of instances on the path
+	int path[PSY_MAX_LEVELS];  // global instance indices, root first
+};
+
+struct Level {
+	int asmb;
+	int stack_base;
+	int shader;
+	int inst;         // global instance that entered this level (-1 for the root)
+	uint64_t id;
+	int id_bits;      // id bits of this level's assembly
+	int inst_base;
+};
+
+// Traces one ray through the scene. Returns the device error flags.
+__device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
+	unsigned err = 0;
+	float max_t = wr.occl ? 1.0f : INFINITY;
+	rec->obj = -1;
+	rec->t = INFINITY;
+	rec->depth = 0;
+
+	Level lv[PSY_MAX_LEVELS];
+	Frame frames[PSY_MAX_LEVELS];  // merged frames of transformed levels
+	int lvl_frame[PSY_MAX_LEVELS];  // frame used by each level, -1 = none
+	int node_stack[PSY_NODE_STACK];
+	int nsp = 0;
+	int L = 0;
+	lv[0].asmb = 0;
+	lv[0].stack_base = 0;
+	lv[0].shader = -1;
+	lv[0].inst = -1;
+	lv[0].id = 0;
+	lv[0].id_bits = sc.assemblies[0].id_bits;
+	lv[0].inst_base = sc.assemblies[0].inst_base;
+	lvl_frame[0] = -1;
+	LocalRay r = make_local(wr);
+	Frame none;
+	none.count = 0;
+
+	{
+		const int root = sc.assemblies[0].root;
+		if (root != REF_EMPTY) node_stack[nsp++] = root;
+	}
+
+	bool done = false;
+	while (!done) {
+		// leave finished levels, restoring the ray of the enclosing level
+		while (L > 0 && nsp == lv[L].stack_base) {
+			const bool changed = lvl_frame[L] != lvl_frame[L - 1];
+			--L;
+			if (changed) {
+				if (lvl_frame[L] >= 0) r = make_local_x(wr, frame_at_index_lerp(frames[lvl_frame[L]], wr.time));
+				else r = make_local(wr);
+			}
+		}
+		if (nsp == 0) break;
+		const int ref = node_stack[--nsp];
+		if (ref >= 0) {
+			// inner node: test the child boxes (BBox4::intersect_ray, basics/bbox.hpp:566-595)
+			const DevNode* nd = sc.nodes + ref;
+			float b[24];
+			const float4* q = reinterpret_cast<const float4*>(nd->b);
+#pragma unroll
+			for (int i = 0; i < 6; ++i) {
+				const float4 v = __ldg(q + i);
+				b[i * 4 + 0] = v.x; b[i * 4 + 1] = v.y; b[i * 4 + 2] = v.z; b[i * 4 + 3] = v.w;
+			}
+			const int4 ch = __ldg(reinterpret_cast<const int4*>(nd->child));
+			const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->nchild));
+			const int nch = meta.x;
+			const int ts = meta.y;
+			if (ts > 1) {
+				const SeqPos sp = seq_pos(wr.time, ts);
+				const float* e0 = sp.i0 == 0 ? nd->b : sc.node_extra + (size_t)(meta.z + sp.i0 - 1) * 24;
+				if (sp.single) {
+					for (int i = 0; i < 24; ++i) b[i] = e0[i];
+				} else {
+					const float* e1 = sc.node_extra + (size_t)(meta.z + sp.i0) * 24;
+					const float ia = one_minus(sp.nalpha);
+					for (int i = 0; i < 24; ++i) b[i] = (e0[i] * ia) + (e1[i] * sp.nalpha);
+				}
+			}
+			const int ds0 = r.dinv.x < 0.0f, ds1 = r.dinv.y < 0.0f, ds2 = r.dinv.z < 0.0f;
+			float tnear[4];
+			int order[4];
+			int nhit = 0;
+			const int chv[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+			for (int c = 0; c < 4; ++c) {
+				const float xlo = (b[(0 + ds0) * 4 + c] - r.o.x) * r.dinv.x;
+				const float xhi = (b[(1 - ds0) * 4 + c] - r.o.x) * r.dinv.x;
+				const float ylo = (b[(2 + ds1) * 4 + c] - r.o.y) * r.dinv.y;
+				const float yhi = (b[(3 - ds1) * 4 + c] - r.o.y) * r.dinv.y;
+				const float zlo = (b[(4 + ds2) * 4 + c] - r.o.z) * r.dinv.z;
+				const float zhi = (b[(5 - ds2) * 4 + c] - r.o.z) * r.dinv.z;
+				const float mins = vmax(vmax(xlo, ylo), vmax(zlo, 0.0f));
+				const float maxs = vmax(vmin(vmin(xhi, yhi), zhi), -INFINITY) * BBOX_MAXT_ADJUST;
+				if (c < nch && mins < max_t && mins <= maxs) {
+					// insertion by near distance (stable for ties)
+					int pos = nhit;
+					while (pos > 0 && tnear[pos - 1] > mins) {
+						tnear[pos] = tnear[pos - 1];
+						order[pos] = order[pos - 1];
+						--pos;
+					}
+					tnear[pos] = mins;
+					order[pos] = chv[c];
+					++nhit;
+				}
+			}
+			if (nsp + nhit > PSY_NODE_STACK) {
+				err |= ERRF_STACK;
+				break;
+			}
+			for (int i = nhit - 1; i >= 0; --i) node_stack[nsp++] = order[i];
+			continue;
+		}
+
+		// leaf: one instance of the current level's assembly
+		const int local = leaf_instance(ref);
+		const int gi = lv[L].inst_base + local;
+		const DevInstance inst = sc.instances[gi];
+		const uint64_t id = id_push(lv[L].id, (uint64_t)local, lv[L].id_bits);
+		const int shader = inst.shader >= 0 ? inst.shader : lv[L].shader;
+		const Frame& parent = lvl_frame[L] >= 0 ? frames[lvl_frame[L]] : none;
+
+		if (inst.kind == INST_ASSEMBLY) {
+			if (L + 1 >= PSY_MAX_LEVELS) {
+				err |= ERRF_LEVELS;
+				continue;
+			}
+			const DevAssembly as = sc.assemblies[inst.data];
+			if (as.root == REF_EMPTY) continue;
+			if (inst.xform_count > 0) {
+				if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &frames[L + 1])) {
+					err |= ERRF_MOTION;
+					continue;
+				}
+				lvl_frame[L + 1] = L + 1;
+				r = make_local_x(wr, frame_at_index_lerp(frames[L + 1], wr.time));
+			} else {
+				lvl_frame[L + 1] = lvl_frame[L];
+			}
+			++L;
+			lv[L].asmb = inst.data;
+			lv[L].stack_base = nsp;
+			lv[L].shader = shader;
+			lv[L].inst = gi;
+			lv[L].id = id;
+			lv[L].id_bits = as.id_bits;
+			lv[L].inst_base = as.inst_base;
+			if (nsp + 1 > PSY_NODE_STACK) {
+				err |= ERRF_STACK;
+				break;
+			}
+			node_stack[nsp++] = as.root;
+			continue;
+		}
+
+		// object instance
+		LocalRay lr = r;
+		if (inst.xform_count > 0) {
+			Frame nf;
+			if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &nf)) {
+				err |= ERRF_MOTION;
+				continue;
+			}
+			lr = make_local_x(wr, frame_at_index_lerp(nf, wr.time));
+		}
+		const DevObject ob = sc.objects[inst.data];
+		bool hit = false;
+		PatchHit ph;
+		ph.u = ph.v = ph.max_dim = 0.0f;
+		if (ob.kind == OBJ_SPHERE || ob.kind == OBJ_SPHERE_LIGHT) {
+			V3 cent;
+			float radi;
+			if (ob.kind == OBJ_SPHERE) {
+				sphere_at(sc, ob, wr.time, &cent, &radi);
+			} else {
+				float col[3];
+				light_at(sc, ob, wr.time, &cent, &radi, col);
+			}
+			const float t = sphere_t(lr.o, lr.d, cent, radi, max_t);
+			if (t >= 0.0f) {
+				hit = true;
+				ph.t = t;
+				if (!wr.occl) max_t = t;
+			}
+		} else if (ob.kind == OBJ_BILINEAR) {
+			const float* v = sc.fpool + ob.data;
+			if (ob.n0 == 1)
+				hit = patch_intersect<4, 1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+			else
+				hit = patch_intersect<4, 2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+		} else if (ob.kind == OBJ_BICUBIC) {
+			const float* v = sc.fpool + ob.data;
+			if (ob.n0 == 1)
+				hit = patch_intersect<16, 1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+			else
+				hit = patch_intersect<16, 2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+		}
+		if (hit) {
+			rec->obj = inst.data;
+			rec->kind = ob.kind;
+			rec->id = id;
+			rec->shader = shader;
+			if (wr.occl) {
+				done = true;
+				break;
+			}
+			rec->t = ph.t;
+			rec->u = ph.u;
+			rec->v = ph.v;
+			rec->max_dim = ph.max_dim;
+			rec->depth = L + 1;
+			for (int k = 1; k <= L; ++k) rec->path[k - 1] = lv[k].inst;
+			rec->path[L] = gi;
+		}
+	}
+	return err;
+}
+
+// Transform from world space into the hit object's space at the ray time
+// (the Intersection::space of the reference), rebuilt from the hit path.
+// Returns false when the path carries no transform (identity).
+__device__ bool hit_space(const DevScene& sc, const HitRec& rec, float time, M44* out, unsigned* err) {
+	Frame f;
+	f.count = 0;
+	for (int k = 0; k < rec.depth; ++k) {
+		const DevInstance inst = sc.instances[rec.path[k]];
+		if (inst.xform_count > 0) {
+			Frame g;
+			if (!frame_merge(f, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &g)) {
+				*err |= ERRF_MOTION;
+				return false;
+			}
+			f = g;
+		}
+	}
+	if (f.count == 0) return false;
+	*out = frame_at_index_lerp(f, time);
+	return true;
+}
+
+}  // namespace psy
+
+#endif
