@@ -279,3 +279,82 @@ class Tracer:
         for f, t in hits.items():
             setattr(hs, f, p(t))
         self.ctx.check(self.ctx.L.psy_trace(self.ctx.h, C.byref(rs), n, C.byref(hs), stream))
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class LightTree:
+    """LightTree::sample over a batch of queries (reference accel/light_tree.cpp:30-96)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def sample(self, q: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        """q: (n, 15) float32 rows n u v pos(3) nor(3) d(3) wavelength time (pad).
+        Returns (out (n, 14) in the oracle's layout: to_light(3) spec(4)
+        hero selection_pdf light_pdf light_count pad(3), ids (n,))."""
+        torch = _torch()
+        dev = torch.device("cuda", self.ctx.device)
+        q = np.ascontiguousarray(q, np.float32).reshape(-1, 15)
+        n = q.shape[0]
+        cols = {"n": q[:, 0], "u": q[:, 1], "v": q[:, 2], "pos": q[:, 3:6], "nor": q[:, 6:9], "d": q[:, 9:12],
+                "wavelength": q[:, 12], "time": q[:, 13]}
+        dq = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in cols.items()}
+        out = {"to_light": torch.zeros((n, 3), dtype=torch.float32, device=dev),
+               "spec": torch.zeros((n, 4), dtype=torch.float32, device=dev),
+               "selection_pdf": torch.zeros(n, dtype=torch.float32, device=dev),
+               "light_pdf": torch.zeros(n, dtype=torch.float32, device=dev),
+               "id": torch.zeros(n, dtype=torch.int64, device=dev)}
+        qs = _abi.LightQuerySoA(*[C.c_void_p(dq[k].data_ptr()) for k in
+                                  ("n", "u", "v", "pos", "nor", "d", "wavelength", "time")])
+        os_ = _abi.LightSampleSoA(*[C.c_void_p(out[k].data_ptr()) for k in
+                                    ("to_light", "spec", "selection_pdf", "light_pdf", "id")])
+        self.ctx.check(self.ctx.L.psy_light_sample(self.ctx.h, C.byref(qs), n, C.byref(os_), None))
+        self.ctx.sync()
+        res = np.zeros((n, 14), np.float32)
+        res[:, 0:3] = out["to_light"].cpu().numpy()
+        res[:, 3:7] = out["spec"].cpu().numpy()
+        res[:, 7] = q[:, 12]
+        res[:, 8] = out["selection_pdf"].cpu().numpy()
+        res[:, 9] = out["light_pdf"].cpu().numpy()
+        return res, out["id"].cpu().numpy().view(np.uint64)
+
+
+class PathTraceIntegrator:
+    """PathTraceIntegrator (reference integrator/path_trace_integrator.hpp:103-126).
+
+    integrate() renders the context's scene and returns the film's per-pixel
+    XYZ sums (h, w, 3) and sample counts (h, w), as the reference's Film
+    accumulates them."""
+
+    def __init__(self, ctx: Context, width: int, height: int, spp: int, seed: int = 1, path_length: int = 4,
+                 stream_paths: int = 0, block_size: int = 0):
+        self.ctx = ctx
+        self.desc = _abi.RenderDesc(width, height, spp, seed, path_length, stream_paths, block_size)
+        self.stats = _abi.RenderStats()
+
+    @classmethod
+    def for_scene(cls, ctx: Context, scene: Scene, **kw):
+        args = dict(width=scene.res_x, height=scene.res_y, spp=scene.spp, seed=scene.seed)
+        args.update(kw)
+        return cls(ctx, **args)
+
+    def integrate_device(self, xyz, counts=None, stream=None) -> None:
+        """Accumulates into device tensors xyz (h*w*3 float32) and counts
+        (h*w int32/uint32), stream-ordered."""
+        self.ctx.check(self.ctx.L.psy_render(self.ctx.h, C.byref(self.desc), C.c_void_p(xyz.data_ptr()),
+                                             C.c_void_p(counts.data_ptr()) if counts is not None else None,
+                                             C.byref(self.stats), stream))
+
+    def integrate(self) -> Tuple[np.ndarray, np.ndarray]:
+        torch = _torch()
+        dev = torch.device("cuda", self.ctx.device)
+        w, h = self.desc.width, self.desc.height
+        xyz = torch.zeros(h * w * 3, dtype=torch.float32, device=dev)
+        cnt = torch.zeros(h * w, dtype=torch.int32, device=dev)
+        self.integrate_device(xyz, cnt)
+        self.ctx.sync()
+        return xyz.cpu().numpy().reshape(h, w, 3), cnt.cpu().numpy().reshape(h, w).astype(np.uint32)

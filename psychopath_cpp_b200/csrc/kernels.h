@@ -29,6 +29,61 @@ struct HitSoA {
 	int want_geometry;  // any geometry field requested
 };
 
+struct HaltonDev {
+	const uint16_t* perm;
+	const uint4* dims;     // base, pow_base, groups, perm_offset
+	const double* cmul;
+};
+
+struct RenderParams {
+	uint32_t width, height, spp, seed, path_length;
+	uint32_t light_count;    // root LightTree::light_count()
+	uint64_t wave_base;      // first global path (sample) index of the wave
+	int wave_paths;          // paths in this wave (a multiple of spp)
+	float min_x, max_x, min_y, max_y;  // film extent (renderer/renderer.cpp:52-55)
+	float ident_inv;         // diagonal of the reference's inverse of the identity
+};
+
+// Path state of one wave, structure of arrays (PTState,
+// integrator/path_trace_integrator.hpp:49-63).
+struct PathSoA {
+	uint32_t* pix;      // x | y << 16
+	uint32_t* smp;      // sampler offset
+	uint32_t* dimstep;  // next sampler dimension | step << 16
+	float* wl;
+	float* time;
+	float* last_pdf;
+	float4* col;
+	float4* fcol;
+	float4* lcol;
+	float* hit;         // stored intersection, 16 floats per path
+	float* pray;        // previous ray, 16 floats per path
+	float* sample;      // film sample XYZ, 3 floats per path
+};
+
+struct WaveQueues {
+	int* q0;
+	int* q1;
+	int* counters;      // per step: live count out, work counter
+	unsigned long long* rays;
+};
+
+struct LightQuerySoADev {
+	const float *n, *u, *v, *pos, *nor, *d, *wavelength, *time;
+};
+struct LightSampleSoADev {
+	float *to_light, *spec, *selection_pdf, *light_pdf;
+	uint64_t* id;
+};
+
+// Persistent grid size for the wavefront step kernels (resident blocks x SMs).
+int render_grid();
+cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
+                               const WaveQueues& wq, float* xyz, uint32_t* counts, unsigned* status, int grid,
+                               cudaStream_t st, uint32_t* launches);
+cudaError_t launch_light_sample(const DevScene& sc, const LightQuerySoADev& q, const LightSampleSoADev& o, uint32_t n,
+                                float ident_inv, unsigned* status, cudaStream_t st);
+
 cudaError_t launch_trace(const DevScene& sc, const RaySoA& rays, const HitSoA& hits, uint32_t n, unsigned* status,
                          cudaStream_t stream);
 

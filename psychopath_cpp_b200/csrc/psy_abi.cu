@@ -10,8 +10,10 @@
 #include <vector>
 
 #include "../../include/psy_b200.h"
+#include "host_cpu.h"
 #include "kernels.h"
 #include "psy_ctx.h"
+#include "sampler_tables.h"
 #include "scene_build.h"
 
 using namespace psy;
@@ -38,6 +40,7 @@ psy_ctx::~psy_ctx() {
 	cudaSetDevice(device);
 	free_scene();
 	for (auto& kv : scratch) cudaFree(kv.second.ptr);
+	for (void* p : const_allocs) cudaFree(p);
 	if (d_status) cudaFree(d_status);
 	if (h_status) cudaFreeHost(h_status);
 }
@@ -115,6 +118,28 @@ int psy_ctx_create(int device, psy_ctx** out) {
 	if (cudaMalloc(&ctx->d_status, sizeof(unsigned)) != cudaSuccess) return PSY_ERR_OOM;
 	if (cudaMemset(ctx->d_status, 0, sizeof(unsigned)) != cudaSuccess) return PSY_ERR_DEVICE;
 	if (cudaMallocHost(&ctx->h_status, sizeof(unsigned)) != cudaSuccess) return PSY_ERR_OOM;
+	// sampler tables, uploaded once per context
+	{
+		const HaltonTables ht = build_halton_tables();
+		std::vector<uint4> dims;
+		for (const HaltonDim& d : ht.dims) dims.push_back(make_uint4(d.base, d.pow_base, d.groups, d.perm_offset));
+		void *p0, *p1, *p2;
+		if (cudaMalloc(&p0, ht.perm.size() * sizeof(uint16_t)) != cudaSuccess) return PSY_ERR_OOM;
+		ctx->const_allocs.push_back(p0);
+		if (cudaMalloc(&p1, dims.size() * sizeof(uint4)) != cudaSuccess) return PSY_ERR_OOM;
+		ctx->const_allocs.push_back(p1);
+		if (cudaMalloc(&p2, ht.cmul.size() * sizeof(double)) != cudaSuccess) return PSY_ERR_OOM;
+		ctx->const_allocs.push_back(p2);
+		if (cudaMemcpy(p0, ht.perm.data(), ht.perm.size() * sizeof(uint16_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+		    cudaMemcpy(p1, dims.data(), dims.size() * sizeof(uint4), cudaMemcpyHostToDevice) != cudaSuccess ||
+		    cudaMemcpy(p2, ht.cmul.data(), ht.cmul.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+			return PSY_ERR_DEVICE;
+		ctx->halton.perm = static_cast<const uint16_t*>(p0);
+		ctx->halton.dims = static_cast<const uint4*>(p1);
+		ctx->halton.cmul = static_cast<const double*>(p2);
+	}
+	ctx->ident_inv = reference_identity_inverse_scale();
+	ctx->render_grid = render_grid();
 	*out = ctx.release();
 	return PSY_OK;
 }
@@ -384,6 +409,102 @@ int psy_trace_host(psy_ctx* ctx, const psy_ray_soa* rays, uint32_t n, const psy_
 			return rc;
 	}
 	return ctx->check_status(st);
+}
+
+
+int psy_light_sample(psy_ctx* ctx, const psy_light_query_soa* q, uint32_t n, const psy_light_sample_soa* out,
+                     void* stream) {
+	if (!ctx || !q || !out) return PSY_ERR_ARG;
+	if (!ctx->has_scene) return ctx_fail(ctx, PSY_ERR_NO_SCENE, "psy_light_sample: no scene uploaded");
+	if (n == 0) return PSY_OK;
+	if (!q->n || !q->u || !q->v || !q->pos || !q->nor || !q->d || !q->wavelength || !q->time)
+		return ctx_fail(ctx, PSY_ERR_ARG, "psy_light_sample: incomplete query arrays");
+	if (ctx->dev.assemblies == nullptr || ctx->host->assemblies[0].light_root < 0)
+		return ctx_fail(ctx, PSY_ERR_ARG, "psy_light_sample: the scene has no lights");
+	cudaSetDevice(ctx->device);
+	LightQuerySoADev qd{q->n, q->u, q->v, q->pos, q->nor, q->d, q->wavelength, q->time};
+	LightSampleSoADev od{out->to_light, out->spec, out->selection_pdf, out->light_pdf, out->id};
+	return ctx_cuda(ctx, launch_light_sample(ctx->dev, qd, od, n, ctx->ident_inv, ctx->d_status, (cudaStream_t)stream),
+	                "light sample launch");
+}
+
+int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* counts, psy_render_stats* stats,
+               void* stream) {
+	if (!ctx || !desc || !xyz) return PSY_ERR_ARG;
+	if (!ctx->has_scene) return ctx_fail(ctx, PSY_ERR_NO_SCENE, "psy_render: no scene uploaded");
+	if (desc->width == 0 || desc->height == 0 || desc->width > 65535 || desc->height > 65535)
+		return ctx_fail(ctx, PSY_ERR_ARG, "psy_render: resolution must be 1..65535 per axis");
+	if (desc->spp == 0 || desc->spp > 65535) return ctx_fail(ctx, PSY_ERR_ARG, "psy_render: spp must be 1..65535");
+	const uint32_t path_length = desc->path_length ? desc->path_length : 4;
+	if (path_length > 40) return ctx_fail(ctx, PSY_ERR_ARG, "psy_render: path_length must be at most 40");
+	if (ctx->host->assemblies[0].light_root < 0)
+		return ctx_fail(ctx, PSY_ERR_ARG, "psy_render: the scene has no lights (the reference integrator needs one)");
+	cudaSetDevice(ctx->device);
+	cudaStream_t st = (cudaStream_t)stream;
+	const uint64_t total = (uint64_t)desc->width * desc->height * desc->spp;
+	uint64_t want = desc->stream_paths ? desc->stream_paths : (1ull << 21);
+	if (want > (1ull << 26)) want = 1ull << 26;
+	uint64_t P = (want / desc->spp) * desc->spp;
+	if (P < desc->spp) P = desc->spp;
+	if (P > total) P = total;
+	int rc;
+	auto buf = [&](const char* name, size_t bytes) -> void* { return ctx->scratch_buffer(name, bytes, &rc); };
+	PathSoA ps;
+	ps.pix = (uint32_t*)buf("r_pix", P * 4);
+	ps.smp = (uint32_t*)buf("r_smp", P * 4);
+	ps.dimstep = (uint32_t*)buf("r_dimstep", P * 4);
+	ps.wl = (float*)buf("r_wl", P * 4);
+	ps.time = (float*)buf("r_time", P * 4);
+	ps.last_pdf = (float*)buf("r_lpdf", P * 4);
+	ps.col = (float4*)buf("r_col", P * 16);
+	ps.fcol = (float4*)buf("r_fcol", P * 16);
+	ps.lcol = (float4*)buf("r_lcol", P * 16);
+	ps.hit = (float*)buf("r_hit", P * 64);
+	ps.pray = (float*)buf("r_pray", P * 64);
+	ps.sample = (float*)buf("r_sample", P * 12);
+	WaveQueues wq;
+	wq.q0 = (int*)buf("r_q0", P * 4);
+	wq.q1 = (int*)buf("r_q1", P * 4);
+	wq.counters = (int*)buf("r_counters", sizeof(int) * 2 * (path_length * 2 + 1));
+	wq.rays = (unsigned long long*)buf("r_rays", sizeof(unsigned long long));
+	if (!ps.pix || !ps.smp || !ps.dimstep || !ps.wl || !ps.time || !ps.last_pdf || !ps.col || !ps.fcol || !ps.lcol ||
+	    !ps.hit || !ps.pray || !ps.sample || !wq.q0 || !wq.q1 || !wq.counters || !wq.rays)
+		return rc ? rc : PSY_ERR_OOM;
+	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(wq.rays, 0, sizeof(unsigned long long), st), "memset"))) return rc;
+	RenderParams rp;
+	rp.width = desc->width;
+	rp.height = desc->height;
+	rp.spp = desc->spp;
+	rp.seed = desc->seed;
+	rp.path_length = path_length;
+	rp.light_count = (uint32_t)ctx->host->assemblies[0].light_count;
+	rp.min_x = -1.0f;
+	rp.max_x = 1.0f;
+	rp.max_y = (float)desc->height / (float)desc->width;
+	rp.min_y = -rp.max_y;
+	rp.ident_inv = ctx->ident_inv;
+	uint32_t launches = 0, waves = 0;
+	for (uint64_t base = 0; base < total; base += P) {
+		rp.wave_base = base;
+		rp.wave_paths = (int)((total - base) < P ? (total - base) : P);
+		if ((rc = ctx_cuda(ctx,
+		                   launch_render_wave(ctx->dev, ctx->halton, rp, ps, wq, xyz, counts, ctx->d_status,
+		                                      ctx->render_grid, st, &launches),
+		                   "render launch")))
+			return rc;
+		++waves;
+	}
+	if (stats) {
+		unsigned long long rays = 0;
+		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(&rays, wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
+			return rc;
+		if ((rc = ctx->check_status(st))) return rc;
+		stats->paths = total;
+		stats->rays = rays;
+		stats->launches = launches;
+		stats->waves = waves;
+	}
+	return PSY_OK;
 }
 
 }  // extern "C"

@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 
+#include "kernels.h"
 #include "psy_scene.h"
 #include "scene_build.h"
 
@@ -33,6 +34,11 @@ struct psy_ctx {
 	unsigned* h_status = nullptr;
 	std::map<std::string, Scratch> scratch;
 	cudaStream_t stream_ = nullptr;
+	// Halton tables (device) and the host CPU's identity-inverse diagonal
+	psy::HaltonDev halton{};
+	std::vector<void*> const_allocs;
+	float ident_inv = 1.0f;
+	int render_grid = 0;
 
 	~psy_ctx();
 	void free_scene();

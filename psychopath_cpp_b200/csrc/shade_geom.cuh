@@ -149,7 +149,7 @@ __device__ __forceinline__ void closure_of_shader(const DevScene& sc, int shader
 
 // Fills the Intersection data of a closest hit. `lo`, `ld` are the ray
 // origin and direction in the hit object's space.
-__device__ void hit_geometry(const DevScene& sc, const HitRec& rec, float time, V3 lo, V3 ld, HitInfo* h) {
+static __device__ void hit_geometry(const DevScene& sc, const HitRec& rec, float time, V3 lo, V3 ld, HitInfo* h) {
 	const DevObject ob = sc.objects[rec.obj];
 	const float t = rec.t;
 	h->light_pdf = 9999.0f;

@@ -419,7 +419,7 @@ struct Level {
 };
 
 // Traces one ray through the scene. Returns the device error flags.
-__device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
+static __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
 	unsigned err = 0;
 	float max_t = wr.occl ? 1.0f : INFINITY;
 	rec->obj = -1;
@@ -630,7 +630,7 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 // Transform from world space into the hit object's space at the ray time
 // (the Intersection::space of the reference), rebuilt from the hit path.
 // Returns false when the path carries no transform (identity).
-__device__ bool hit_space(const DevScene& sc, const HitRec& rec, float time, M44* out, unsigned* err) {
+static __device__ bool hit_space(const DevScene& sc, const HitRec& rec, float time, M44* out, unsigned* err) {
 	Frame f;
 	f.count = 0;
 	for (int k = 0; k < rec.depth; ++k) {

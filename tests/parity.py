@@ -60,9 +60,14 @@ def concat_rays(*rs) -> dict:
     return {k: np.concatenate([r[k] for r in rs]) for k in rs[0]}
 
 
-def compare_trace(ref: dict, mine: dict, types: np.ndarray) -> dict:
+def compare_trace(ref: dict, mine: dict, types: np.ndarray, uv_mask=None) -> dict:
     """Compares reference (oracle) and CUDA hits; returns counts of each
-    kind of disagreement plus the near-tie count."""
+    kind of disagreement plus the near-tie count.
+
+    `uv_mask` selects the rays whose uv is compared.  The reference leaves
+    Intersection fields that a closer hit does not write (uv of a light hit,
+    light_pdf of a surface hit) holding values from farther candidates, so
+    uv is only meaningful for surface hits."""
     occl = types == 32
     rh = ref["hit"].astype(bool)
     mh = mine["hit"].astype(bool)
@@ -81,7 +86,8 @@ def compare_trace(ref: dict, mine: dict, types: np.ndarray) -> dict:
     rep["t_ulp_max"] = int(tu.max()) if tu.size else 0
     rep["t_over"] = int((tu > T_ULP).sum())
     if "uv" in ref and "uv" in mine:
-        uu = ulp_diff(ref["uv"][both][ids_eq], mine["uv"][both][ids_eq])
+        sel = ids_eq if uv_mask is None else ids_eq & uv_mask[both]
+        uu = ulp_diff(ref["uv"][both][sel], mine["uv"][both][sel])
         rep["uv_ulp_max"] = int(uu.max()) if uu.size else 0
         rep["uv_over"] = int((uu > UV_ULP).sum())
     return rep
