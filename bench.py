@@ -3,6 +3,11 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload trace|render] [--impl ours|reference]
 
 Workloads (seeded synthetic inputs; no public scene set exists):
+  render  (default) the many-light 720p render: 1280x720, 64 spp, 6 path
+          segments; 2,000 bicubic patches, 500 sphere groups instanced through
+          3 assembly levels with transform motion, 10,000 sphere lights sampled
+          through the light tree with MIS, depth of field and camera motion.
+          A step renders the whole frame (58,982,400 paths).
   trace   ray-stream trace microbenchmark: 4,194,304 rays (half Morton-coherent,
           half shuffled, cosine about -z) against a 256x256 bilinear-patch fBm
           heightfield diced to 8x8 cells per patch; a step traces all rays
@@ -31,6 +36,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CLOSEST_RAY = 80  # 60 B read (o, d, t_max, time, ray width, id/flags) + 20 B written (id 8, t, u, v)
+BYTES_PER_PATH_EXTRA = 20   # sampler seed 4 + pixel 4 + XYZ 12
+RENDER_RES = (1280, 720)
+RENDER_SPP = 64
+RENDER_PATH_LENGTH = 6
 HEIGHTFIELD_N = 256
 TRACE_RAYS = 4194304
 
@@ -224,6 +233,141 @@ def trace_cpu_baseline(seconds_target: float = 10.0):
                       "best of 3" % threads}
 
 
+# --------------------------------------------------------------------------
+# render workload
+# --------------------------------------------------------------------------
+
+def render_workload():
+    from psychopath_cpp_b200 import scenes
+    return scenes.many_light_scene(3, res=RENDER_RES, spp=RENDER_SPP)
+
+
+RENDER_METRIC = "paths/s at 720p (1280x720, 64 spp, 6 segments, many-light scene)"
+RENDER_WORKLOAD = ("render: 1280x720 x 64 spp, 6 segments; 2,000 bicubic patches, 500 sphere groups through 3 "
+                   "assembly levels with transform motion, 10,000 sphere lights (light tree + MIS), DoF, camera motion")
+
+
+def run_render_ours(args, rank, local, pg, world):
+    import torch
+    from psychopath_cpp_b200 import api
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sc = render_workload()
+    ctx = api.Context(local)
+    ctx.upload(sc)
+    w, h = RENDER_RES
+    integ = api.PathTraceIntegrator(ctx, w, h, RENDER_SPP, seed=1, path_length=RENDER_PATH_LENGTH,
+                                    stream_paths=args.stream_paths)
+    xyz = torch.zeros(w * h * 3, dtype=torch.float32, device=dev)
+    cnt = torch.zeros(w * h, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    for _ in range(args.warmup):
+        integ.integrate_device(xyz, cnt, sp, with_stats=False)
+    integ.integrate_device(xyz, cnt, sp, with_stats=True)  # rays and launches of one render
+    rays_per_render = int(integ.stats.rays)
+    launches_per_render = int(integ.stats.launches)
+    paths = w * h * RENDER_SPP
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            integ.integrate_device(xyz, cnt, sp, with_stats=False)
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+    ctx.sync(sp)
+    if pg:
+        pg.barrier()
+    ms = start.elapsed_time(end) / args.steps
+    ms = max_over_ranks(ms, pg, dev)
+    value = world * paths / (ms * 1e-3)
+    mrays = world * rays_per_render / (ms * 1e-3) / 1e6
+    rbar = rays_per_render / paths
+    bytes_per_path = rbar * BYTES_PER_CLOSEST_RAY + BYTES_PER_PATH_EXTRA
+    hbm, peak_kind = measured_peaks()
+    achieved = bytes_per_path * paths / (ms * 1e-3) / 1e9
+    # end to end: the public call plus the device->host read of the film each step
+    h_xyz = torch.empty(w * h * 3, dtype=torch.float32, pin_memory=True)
+    h_cnt = torch.empty(w * h, dtype=torch.int32, pin_memory=True)
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    e2e_steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        integ.integrate_device(xyz, cnt, sp, with_stats=False)
+        h_xyz.copy_(xyz, non_blocking=True)
+        h_cnt.copy_(cnt, non_blocking=True)
+        torch.cuda.synchronize(dev)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    e2e_ms = max_over_ranks(e2e_ms, pg, dev)
+    ctx.sync(sp)
+    return {
+        "metric": RENDER_METRIC, "value": round(value, 1), "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded many-light scene)",
+        "config": {"workload": RENDER_WORKLOAD, "paths_per_step": paths, "path_length": RENDER_PATH_LENGTH,
+                   "stream_paths": args.stream_paths or "auto (2^21)",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "per-path state (~200 B x 2M paths in flight) larger than L2"},
+        "mrays_per_s": round(mrays, 2), "rays_per_path": round(rbar, 4),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 5), "traffic": None, "peak_source": peak_kind,
+                     "basis": "R*80 + 20 B per path (R = rays per path)"},
+        "e2e": {"value": round(world * paths / (e2e_ms * 1e-3), 1), "unit": "paths/s",
+                "h2d_bytes_per_step": 28, "d2h_bytes_per_step": w * h * 16},
+        "gpu_launches": launches_per_render * args.steps,
+        "clocks": clk.summary(),
+    }
+
+
+def render_cpu_baseline(spp: int = 4):
+    """The reference's PathTraceIntegrator::integrate (oracle/_ref) on this
+    host's cores over a bounded sample of the render: the full frame at a
+    few samples per pixel."""
+    from oracle import psyref
+    if not psyref.available():
+        return None
+    ref = psyref.RefScene(scene=render_workload())
+    threads = os.cpu_count() or 1
+    xyz, cnt, rays, secs = ref.render(threads=threads, spp=spp, path_length=RENDER_PATH_LENGTH, seed=1)
+    paths = RENDER_RES[0] * RENDER_RES[1] * spp
+    return {"value": round(paths / secs, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
+            "mrays_per_s": round(rays / secs / 1e6, 3),
+            "sample": "the 1280x720 frame at %d spp (%d paths) instead of 64, PathTraceIntegrator::integrate on "
+                      "%d threads" % (spp, paths, threads)}
+
+
+def run_render_reference(args, spp: int = 2):
+    from oracle import psyref
+    if not psyref.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libpsyref.so (the reference built from source) is missing"}
+    ref = psyref.RefScene(scene=render_workload())
+    threads = os.cpu_count() or 1
+    paths = RENDER_RES[0] * RENDER_RES[1] * spp
+    for _ in range(args.warmup):
+        ref.render(threads=threads, spp=spp, path_length=RENDER_PATH_LENGTH, seed=1)
+    tot, rays = 0.0, 0
+    for _ in range(args.steps):
+        _, _, r, secs = ref.render(threads=threads, spp=spp, path_length=RENDER_PATH_LENGTH, seed=1)
+        tot += secs
+        rays += r
+    ms = tot * 1e3 / args.steps
+    value = paths / (ms * 1e-3)
+    return {"metric": RENDER_METRIC, "impl": "reference", "value": round(value, 1), "unit": "paths/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded many-light scene)",
+            "config": {"workload": RENDER_WORKLOAD, "sample_paths_per_step": paths},
+            "mrays_per_s": round(rays / tot / 1e6, 3),
+            "cpu_baseline": {"value": round(value, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
+                             "sample": "the 1280x720 frame at %d spp per step (%d paths), PathTraceIntegrator::"
+                                       "integrate on %d threads" % (spp, paths, threads)},
+            "e2e": {"value": round(value, 1), "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_trace_reference(args):
     from oracle import psyref
     if not psyref.available():
@@ -258,7 +402,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="trace", choices=["trace"])
+    ap.add_argument("--workload", default="render", choices=["render", "trace"])
+    ap.add_argument("--stream-paths", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -266,15 +411,19 @@ def main():
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_trace_reference(args)))
+            fn = run_render_reference if args.workload == "render" else run_trace_reference
+            print(json.dumps(fn(args)))
         if pg:
             pg.barrier()
             pg.destroy_process_group()
         return
-    res = run_trace_ours(args, rank, local, pg, world)
+    if args.workload == "render":
+        res = run_render_ours(args, rank, local, pg, world)
+    else:
+        res = run_trace_ours(args, rank, local, pg, world)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            res["cpu_baseline"] = trace_cpu_baseline()
+            res["cpu_baseline"] = render_cpu_baseline() if args.workload == "render" else trace_cpu_baseline()
         print(json.dumps(res))
     if pg:
         pg.barrier()

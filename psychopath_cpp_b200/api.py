@@ -342,12 +342,13 @@ class PathTraceIntegrator:
         args.update(kw)
         return cls(ctx, **args)
 
-    def integrate_device(self, xyz, counts=None, stream=None) -> None:
+    def integrate_device(self, xyz, counts=None, stream=None, with_stats: bool = True) -> None:
         """Accumulates into device tensors xyz (h*w*3 float32) and counts
-        (h*w int32/uint32), stream-ordered."""
+        (h*w int32/uint32), stream-ordered.  With with_stats the call also
+        synchronises the stream and fills self.stats (rays, launches)."""
         self.ctx.check(self.ctx.L.psy_render(self.ctx.h, C.byref(self.desc), C.c_void_p(xyz.data_ptr()),
                                              C.c_void_p(counts.data_ptr()) if counts is not None else None,
-                                             C.byref(self.stats), stream))
+                                             C.byref(self.stats) if with_stats else None, stream))
 
     def integrate(self) -> Tuple[np.ndarray, np.ndarray]:
         torch = _torch()
