@@ -57,7 +57,7 @@ def lib():
         L.psyref_lighttree_bounds_count.restype = sz
         L.psyref_lighttree_bounds_count.argtypes = [vp, C.c_int]
         L.psyref_lighttree_nodes.argtypes = [vp, C.c_int, u64p, fp, fp]
-        L.psyref_lighttree_totals.argtypes = [vp, u64p, fp]
+        L.psyref_lighttree_totals.argtypes = [vp, C.c_int, u64p, fp]
         _lib = L
     return _lib
 
@@ -184,7 +184,7 @@ class RefScene:
                                          _p(bb, C.c_float))
         cnt = C.c_uint64()
         tot = C.c_float()
-        lib().psyref_lighttree_totals(self.h, C.byref(cnt), C.byref(tot))
+        lib().psyref_lighttree_totals(self.h, assembly, C.byref(cnt), C.byref(tot))
         return {"meta": meta, "energy": en, "bounds": bb[:nb], "light_count": cnt.value, "total_energy": tot.value}
 
 

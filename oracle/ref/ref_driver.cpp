@@ -483,9 +483,9 @@ void psyref_lighttree_nodes(void* h, int assembly, uint64_t* meta, float* energy
 	}
 }
 
-/* LightTree totals of the root assembly: light_count, total energy. */
-void psyref_lighttree_totals(void* h, uint64_t* count, float* energy) {
-	const auto& lt = static_cast<RefScene*>(h)->scene->root->light_accel;
+/* LightTree totals of one assembly: light_count, total energy. */
+void psyref_lighttree_totals(void* h, int assembly, uint64_t* count, float* energy) {
+	const auto& lt = static_cast<RefScene*>(h)->assemblies[assembly]->light_accel;
 	*count = lt.light_count();
 	*energy = lt_view(lt).total_energy;
 }

@@ -1,0 +1,53 @@
+"""The C ABI library: it loads, exports every function include/psy_b200.h
+declares, and reports errors through return codes (no GPU needed)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from psychopath_cpp_b200 import _abi
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "psy_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(psy_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_expected_surface():
+    fns = declared_functions()
+    for f in ("psy_trace", "psy_scene_upload", "psy_render", "psy_light_sample"):
+        assert f in fns
+    assert set(_abi.EXPORTED) <= set(fns)
+
+
+def test_library_exports_every_declared_symbol():
+    L = _abi.load()
+    missing = [f for f in declared_functions() if not hasattr(L, f)]
+    assert not missing, missing
+
+
+def test_version_and_null_arguments():
+    L = _abi.load()
+    assert L.psy_version().startswith(b"psy_b200")
+    assert L.psy_ctx_create(0, None) == _abi.PSY_ERR_ARG
+    assert L.psy_last_error(None) == b"no context"
+    assert L.psy_scene_upload(None, None) == _abi.PSY_ERR_ARG
+    assert L.psy_trace(None, None, 0, None, None) == _abi.PSY_ERR_ARG
+    assert L.psy_sync(None, None) == _abi.PSY_ERR_ARG
+
+
+def test_context_creation_without_a_device_fails_cleanly():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a CUDA device is present")
+    except ImportError:
+        pass
+    L = _abi.load()
+    h = C.c_void_p()
+    assert L.psy_ctx_create(0, C.byref(h)) == _abi.PSY_ERR_DEVICE
+    assert not h.value
