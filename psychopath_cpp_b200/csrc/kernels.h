@@ -77,7 +77,7 @@ struct LightSampleSoADev {
 };
 
 // Persistent grid size for the wavefront step kernels (resident blocks x SMs).
-int render_grid();
+int render_grid(unsigned features);
 cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
                                const WaveQueues& wq, float* xyz, uint32_t* counts, unsigned* status, int grid,
                                cudaStream_t st, uint32_t* launches);

@@ -139,7 +139,6 @@ int psy_ctx_create(int device, psy_ctx** out) {
 		ctx->halton.cmul = static_cast<const double*>(p2);
 	}
 	ctx->ident_inv = reference_identity_inverse_scale();
-	ctx->render_grid = render_grid();
 	*out = ctx.release();
 	return PSY_OK;
 }
@@ -181,6 +180,7 @@ int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* desc) {
 #undef UP
 	d.assembly_count = (int)b->assemblies.size();
 	d.max_depth = b->max_depth;
+	d.features = b->features;
 	d.dice_rate = b->dice_rate;
 	d.min_upoly_size = b->min_upoly_size;
 	d.cam_xform_count = (int)b->cam_xforms.size() / 16;
@@ -484,12 +484,13 @@ int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* 
 	rp.min_y = -rp.max_y;
 	rp.ident_inv = ctx->ident_inv;
 	uint32_t launches = 0, waves = 0;
+	const int grid = render_grid(ctx->dev.features);
 	for (uint64_t base = 0; base < total; base += P) {
 		rp.wave_base = base;
 		rp.wave_paths = (int)((total - base) < P ? (total - base) : P);
 		if ((rc = ctx_cuda(ctx,
-		                   launch_render_wave(ctx->dev, ctx->halton, rp, ps, wq, xyz, counts, ctx->d_status,
-		                                      ctx->render_grid, st, &launches),
+		                   launch_render_wave(ctx->dev, ctx->halton, rp, ps, wq, xyz, counts, ctx->d_status, grid,
+		                                      st, &launches),
 		                   "render launch")))
 			return rc;
 		++waves;

@@ -38,7 +38,6 @@ struct psy_ctx {
 	psy::HaltonDev halton{};
 	std::vector<void*> const_allocs;
 	float ident_inv = 1.0f;
-	int render_grid = 0;
 
 	~psy_ctx();
 	void free_scene();

@@ -31,6 +31,16 @@ enum : int { CLOSURE_NONE = 0, CLOSURE_LAMBERT = 1, CLOSURE_EMIT = 2, CLOSURE_GT
 // Device error flags, OR-ed into the context's status word by kernels.
 enum : unsigned { ERRF_STACK = 1u, ERRF_LEVELS = 2u, ERRF_MOTION = 4u, ERRF_TIMEOUT = 8u, ERRF_NOLIGHT = 16u };
 
+// Scene features that select a compiled variant of the traversal kernels.
+enum : unsigned {
+	FEAT_NESTED = 1u,        // assembly instances (levels)
+	FEAT_XFORM = 2u,         // instance transforms
+	FEAT_BICUBIC = 4u,       // bicubic patches
+	FEAT_PATCH_MOTION = 8u,  // patches with two time samples
+	FEAT_FLAT = 0u,
+	FEAT_ALL = 15u
+};
+
 // A child reference in a BVH4 node or an assembly root:
 //   >= 0          inner node index (global)
 //   < 0, != EMPTY leaf: local instance index = -(ref + 1)
@@ -105,6 +115,7 @@ struct DevScene {
 	const DevShader* shaders;
 	int assembly_count;
 	int max_depth;        // deepest assembly nesting (root = 1)
+	unsigned features;    // FEAT_* present in the scene
 	float dice_rate;
 	float min_upoly_size;
 	// camera

@@ -70,10 +70,11 @@ __device__ __forceinline__ void store_hit(const PathSoA& ps, int s, const Stored
 // Intersection -> stored hit: DifferentialGeometry::transformed_from(space)
 // (basics/differential_geometry.hpp:20-40) and the offset of
 // path_trace_integrator.cpp:141-145.
+template <unsigned F>
 __device__ void make_stored(const DevScene& sc, const HitRec& rec, const WorldRayD& wr, float ident_inv,
                             StoredHit* sh, int* closure, float* emit_col, float* light_pdf, unsigned* err) {
 	M44 space;
-	const bool xf = hit_space(sc, rec, wr.time, &space, err);
+	const bool xf = hit_space<F>(sc, rec, wr.time, &space, err);
 	V3 lo = wr.o, ld = wr.d;
 	if (xf) {
 		lo = pos_to(space, wr.o);
@@ -134,7 +135,7 @@ __device__ __forceinline__ void finish_path(const RenderParams& rp, const PathSo
 	reinterpret_cast<float3*>(ps.sample)[slot] = o;
 }
 
-template <int KIND>
+template <int KIND, unsigned F>
 __global__ void __launch_bounds__(128) step_kernel(DevScene sc, HaltonDev hd, RenderParams rp, PathSoA ps,
                                                   const int* __restrict__ q_in, const int* n_in, int* q_out,
                                                   int* n_out, int* work, unsigned long long* ray_count,
@@ -204,13 +205,13 @@ __global__ void __launch_bounds__(128) step_kernel(DevScene sc, HaltonDev hd, Re
 				camera_ray(sc, rx, ry, dx, dy, samp_c, samp_a, samp_b, &wr);
 				time = wr.time;
 				HitRec rec;
-				err |= trace_ray(sc, wr, &rec);
+				err |= trace_ray<F>(sc, wr, &rec);
 				++rays;
 				// update_path for a camera ray (path_trace_integrator.cpp:251-272)
 				if (rec.obj >= 0) {
 					int closure;
 					float ecol[3], lpdf;
-					make_stored(sc, rec, wr, rp.ident_inv, &sh, &closure, ecol, &lpdf, &err);
+					make_stored<F>(sc, rec, wr, rp.ident_inv, &sh, &closure, ecol, &lpdf, &err);
 					if (closure == CLOSURE_EMIT) {
 						done = true;
 						const Spec e = rgb_to_spec(ecol, wl);
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(128) step_kernel(DevScene sc, HaltonDev hd, Re
 					wr.occl = true;
 					propagate_differentials(sh, &wr);
 					HitRec rec;
-					err |= trace_ray(sc, wr, &rec);
+					err |= trace_ray<F>(sc, wr, &rec);
 					++rays;
 					// update_path, shadow result (path_trace_integrator.cpp:235-249)
 					if (rec.obj < 0) {
@@ -284,13 +285,13 @@ __global__ void __launch_bounds__(128) step_kernel(DevScene sc, HaltonDev hd, Re
 				for (int k = 0; k < 4; ++k) fcol.e[k] *= filter.e[k] / pdf;
 				last_pdf = pdf;
 				HitRec rec;
-				err |= trace_ray(sc, wr, &rec);
+				err |= trace_ray<F>(sc, wr, &rec);
 				++rays;
 				if (rec.obj >= 0) {
 					int closure;
 					float ecol[3], lpdf;
 					StoredHit nh;
-					make_stored(sc, rec, wr, rp.ident_inv, &nh, &closure, ecol, &lpdf, &err);
+					make_stored<F>(sc, rec, wr, rp.ident_inv, &nh, &closure, ecol, &lpdf, &err);
 					if (closure == CLOSURE_EMIT) {
 						done = true;
 						const Spec e = rgb_to_spec(ecol, wl);
@@ -380,13 +381,14 @@ __global__ void film_reduce_kernel(RenderParams rp, PathSoA ps, float* xyz, uint
 	if (counts) counts[pixel] += c;
 }
 
-int render_grid() {
+template <unsigned F>
+static int grid_for() {
 	int dev = 0, sms = 0, b0 = 0, b1 = 0, b2 = 0;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, step_kernel<STEP_CAMERA>, 128, 0);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, step_kernel<STEP_SHADOW>, 128, 0);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, step_kernel<STEP_BOUNCE>, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, step_kernel<STEP_CAMERA, F>, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, step_kernel<STEP_SHADOW, F>, 128, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, step_kernel<STEP_BOUNCE, F>, 128, 0);
 	int b = b0;
 	if (b1 > 0 && b1 < b) b = b1;
 	if (b2 > 0 && b2 < b) b = b2;
@@ -394,13 +396,11 @@ int render_grid() {
 	return sms * b;
 }
 
-cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
-                               const WaveQueues& wq, float* xyz, uint32_t* counts, unsigned* status, int grid,
-                               cudaStream_t st, uint32_t* launches) {
-	const int block = 128;
-	pix_init_kernel<<<(rp.wave_paths + 255) / 256, 256, 0, st>>>(rp, ps);
-	++*launches;
-	cudaMemsetAsync(wq.counters, 0, sizeof(int) * 2 * (rp.path_length * 2 + 1), st);
+int render_grid(unsigned features) { return features == FEAT_FLAT ? grid_for<FEAT_FLAT>() : grid_for<FEAT_ALL>(); }
+
+template <unsigned F>
+static void launch_steps(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
+                         const WaveQueues& wq, unsigned* status, int grid, cudaStream_t st, uint32_t* launches) {
 	int* n_prev = nullptr;
 	const int* q_prev = nullptr;
 	for (int s = 0; s < (int)rp.path_length * 2; ++s) {
@@ -408,18 +408,28 @@ cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const Re
 		int* n_out = wq.counters + 2 * s;
 		int* work = wq.counters + 2 * s + 1;
 		if (s == 0)
-			step_kernel<STEP_CAMERA><<<grid, block, 0, st>>>(sc, hd, rp, ps, nullptr, nullptr, q_out, n_out, work,
-			                                                  wq.rays, status);
+			step_kernel<STEP_CAMERA, F><<<grid, 128, 0, st>>>(sc, hd, rp, ps, nullptr, nullptr, q_out, n_out, work,
+			                                                   wq.rays, status);
 		else if (s & 1)
-			step_kernel<STEP_SHADOW><<<grid, block, 0, st>>>(sc, hd, rp, ps, q_prev, n_prev, q_out, n_out, work,
-			                                                  wq.rays, status);
+			step_kernel<STEP_SHADOW, F><<<grid, 128, 0, st>>>(sc, hd, rp, ps, q_prev, n_prev, q_out, n_out, work,
+			                                                   wq.rays, status);
 		else
-			step_kernel<STEP_BOUNCE><<<grid, block, 0, st>>>(sc, hd, rp, ps, q_prev, n_prev, q_out, n_out, work,
-			                                                  wq.rays, status);
+			step_kernel<STEP_BOUNCE, F><<<grid, 128, 0, st>>>(sc, hd, rp, ps, q_prev, n_prev, q_out, n_out, work,
+			                                                   wq.rays, status);
 		++*launches;
 		q_prev = q_out;
 		n_prev = n_out;
 	}
+}
+
+cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
+                               const WaveQueues& wq, float* xyz, uint32_t* counts, unsigned* status, int grid,
+                               cudaStream_t st, uint32_t* launches) {
+	pix_init_kernel<<<(rp.wave_paths + 255) / 256, 256, 0, st>>>(rp, ps);
+	++*launches;
+	cudaMemsetAsync(wq.counters, 0, sizeof(int) * 2 * (rp.path_length * 2 + 1), st);
+	if (sc.features == FEAT_FLAT) launch_steps<FEAT_FLAT>(sc, hd, rp, ps, wq, status, grid, st, launches);
+	else launch_steps<FEAT_ALL>(sc, hd, rp, ps, wq, status, grid, st, launches);
 	film_reduce_kernel<<<(rp.wave_paths / rp.spp + 127) / 128, 128, 0, st>>>(rp, ps, xyz, counts);
 	++*launches;
 	return cudaGetLastError();

@@ -753,6 +753,16 @@ struct Builder {
 			}
 		}
 		out->max_depth = finalize(0, 1);
+		// kernel variant selection
+		for (const DevInstance& di : out->instances) {
+			if (di.kind == INST_ASSEMBLY) out->features |= FEAT_NESTED;
+			if (di.xform_count > 0) out->features |= FEAT_XFORM;
+		}
+		for (const DevObject& ob : out->objects) {
+			if (ob.kind == OBJ_BICUBIC) out->features |= FEAT_BICUBIC;
+			if ((ob.kind == OBJ_BILINEAR || ob.kind == OBJ_BICUBIC) && ob.n0 > 1) out->features |= FEAT_PATCH_MOTION;
+			if ((ob.kind == OBJ_BILINEAR || ob.kind == OBJ_BICUBIC) && ob.n0 > 2) return fail("patches support at most two time samples");
+		}
 		out->total_lights = asms[0].light_count;
 		for (uint32_t s = 0; s < desc->shader_count; ++s) {
 			DevShader ds{};

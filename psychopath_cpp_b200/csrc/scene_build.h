@@ -38,6 +38,7 @@ struct BuiltScene {
 	float dice_rate = 0.25f;
 	float min_upoly_size = 0.00001f;
 	int max_depth = 1;
+	unsigned features = 0;  // FEAT_* present
 	uint32_t total_lights = 0;
 	std::vector<RefBVH4> ref_bvh4;    // per assembly
 };

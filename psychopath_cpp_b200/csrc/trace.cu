@@ -18,6 +18,7 @@ __device__ __forceinline__ void st3(float* p, uint32_t i, V3 v) {
 	p[3 * (size_t)i + 2] = v.z;
 }
 
+template <unsigned F>
 __global__ void __launch_bounds__(128) trace_kernel(DevScene sc, RaySoA rays, HitSoA hits, uint32_t n,
                                                    unsigned* status) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -33,14 +34,14 @@ __global__ void __launch_bounds__(128) trace_kernel(DevScene sc, RaySoA rays, Hi
 	wr.occl = rays.type ? (__ldg(rays.type + i) == 32) : false;
 
 	HitRec rec;
-	unsigned err = trace_ray(sc, wr, &rec);
+	unsigned err = trace_ray<F>(sc, wr, &rec);
 	const bool hit = rec.obj >= 0;
 	if (hits.hit) hits.hit[i] = hit ? 1 : 0;
 	if (hits.id) hits.id[i] = hit ? rec.id : 0ull;
 	if (hits.t) hits.t[i] = (hit && !wr.occl) ? rec.t : INFINITY;
 	if (hit && !wr.occl && hits.want_geometry) {
 		M44 space;
-		const bool xf = hit_space(sc, rec, wr.time, &space, &err);
+		const bool xf = hit_space<F>(sc, rec, wr.time, &space, &err);
 		V3 lo = wr.o, ld = wr.d;
 		if (xf) {
 			lo = pos_to(space, wr.o);
@@ -99,7 +100,10 @@ cudaError_t launch_trace(const DevScene& sc, const RaySoA& rays, const HitSoA& h
 	if (n == 0) return cudaSuccess;
 	const int block = 128;
 	const uint32_t grid = (n + block - 1) / block;
-	trace_kernel<<<grid, block, 0, stream>>>(sc, rays, hits, n, status);
+	if (sc.features == FEAT_FLAT)
+		trace_kernel<FEAT_FLAT><<<grid, block, 0, stream>>>(sc, rays, hits, n, status);
+	else
+		trace_kernel<FEAT_ALL><<<grid, block, 0, stream>>>(sc, rays, hits, n, status);
 	return cudaGetLastError();
 }
 

@@ -394,6 +394,144 @@ __device__ bool patch_intersect(const float* verts, float time, const LocalRay& 
 	return found;
 }
 
+// Bilinear patches: the same depth-first bisection without a stack of
+// sub-patches.  A node is identified by its path from the root (one bit per
+// split: 1 = second half, visited first) and the split direction taken at
+// each level; when a subtree is finished, the deepest pending first half is
+// rebuilt by replaying the recorded splits from the root.  Replaying runs
+// the same float operations in the same order as the original descent, so
+// every node's control points and uv range are bit-identical to the stored
+// ones, and the per-ray state stays in registers.  The reference's stack
+// index (its forced-leaf limit of 63) counts second halves only, which is
+// the population count of the path.
+struct Bits128 {
+	uint64_t lo, hi;
+	__device__ __forceinline__ bool get(int i) const { return i < 64 ? ((lo >> i) & 1ull) : ((hi >> (i - 64)) & 1ull); }
+	__device__ __forceinline__ void set(int i, bool v) {
+		if (i < 64) lo = v ? (lo | (1ull << i)) : (lo & ~(1ull << i));
+		else hi = v ? (hi | (1ull << (i - 64))) : (hi & ~(1ull << (i - 64)));
+	}
+	// keep bits [0, n)
+	__device__ __forceinline__ void truncate(int n) {
+		if (n <= 0) { lo = 0; hi = 0; }
+		else if (n < 64) { lo &= (1ull << n) - 1ull; hi = 0; }
+		else if (n < 128) { hi &= (1ull << (n - 64)) - 1ull; }
+	}
+	// highest set bit below n, or -1
+	__device__ __forceinline__ int highest_below(int n) const {
+		Bits128 t = *this;
+		t.truncate(n);
+		if (t.hi) return 64 + 63 - __clzll((long long)t.hi);
+		if (t.lo) return 63 - __clzll((long long)t.lo);
+		return -1;
+	}
+	__device__ __forceinline__ int popc() const { return __popcll(lo) + __popcll(hi); }
+};
+
+template <int TSC>
+__device__ bool bilinear_intersect(const float* verts, float time, const LocalRay& r, float* max_t, bool occl,
+                                   float dice_rate, float min_upoly, PatchHit* hit) {
+	Patch<4> root[TSC], cur[TSC];
+#pragma unroll
+	for (int k = 0; k < TSC; ++k) {
+		patch_load<4>(verts + k * 12, &root[k]);
+		cur[k] = root[k];
+	}
+	int t_index = 0;
+	float t_nalpha = 0.0f;
+	if (TSC > 1) {
+		const float t_time = time * (float)(TSC - 1);
+		t_index = (int)t_time;
+		t_nalpha = t_time - (float)t_index;
+		if (t_index > TSC - 2) t_index = TSC - 2;
+	}
+	Bits128 path{0, 0}, dirs{0, 0};  // dirs bit: 1 = split along u
+	int depth = 0;                   // splits from the root
+	float u0 = 0.0f, u1 = 1.0f, v0 = 0.0f, v1 = 1.0f;
+	bool found = false;
+	while (true) {
+		Box bb[TSC];
+		float max_dim = 0.0f;
+#pragma unroll
+		for (int k = 0; k < TSC; ++k) {
+			bb[k] = patch_bound<4>(cur[k]);
+			const float ld = longest_axis(bb[k].hi - bb[k].lo);
+			max_dim = (k == 0) ? ld : smax(max_dim, ld);
+		}
+		float h0, h1;
+		bool h;
+		if (TSC == 1) h = box_hit(bb[0], r.o, r.dinv, *max_t, &h0, &h1);
+		else h = box_hit(box_lerp(t_nalpha, bb[t_index], bb[t_index + 1]), r.o, r.dinv, *max_t, &h0, &h1);
+		bool descend = false;
+		if (h) {
+			const float width = smax(ray_min_width(r.w, h0, h1) * dice_rate, min_upoly);
+			if (max_dim <= width || path.popc() == PSY_SPLIT_STACK - 1 || depth == 127) {
+				const float tt = (h0 + h1) * 0.5f;
+				if (tt > 0.0f && tt < *max_t) {
+					found = true;
+					if (occl) return true;
+					*max_t = tt;
+					hit->t = tt;
+					hit->u = (u0 + u1) * 0.5f;
+					hit->v = (v0 + v1) * 0.5f;
+					hit->max_dim = max_dim;
+				}
+			} else {
+				descend = true;
+			}
+		}
+		if (descend) {
+			Patch<4> second[TSC];
+			const bool along_u = patch_ulen(cur[0]) > patch_vlen(cur[0]);
+			if (along_u) {
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) patch_split_u(cur[k], &second[k]);
+				u0 = (u0 + u1) * 0.5f;
+			} else {
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) patch_split_v(cur[k], &second[k]);
+				v0 = (v0 + v1) * 0.5f;
+			}
+#pragma unroll
+			for (int k = 0; k < TSC; ++k) cur[k] = second[k];
+			path.set(depth, true);
+			dirs.set(depth, along_u);
+			++depth;
+			continue;
+		}
+		// the deepest pending first half
+		const int lvl = path.highest_below(depth);
+		if (lvl < 0) break;
+		path.set(lvl, false);
+		depth = lvl + 1;
+		path.truncate(depth);
+		dirs.truncate(depth);
+#pragma unroll
+		for (int k = 0; k < TSC; ++k) cur[k] = root[k];
+		u0 = 0.0f; u1 = 1.0f; v0 = 0.0f; v1 = 1.0f;
+		for (int j = 0; j < depth; ++j) {
+			const bool second_half = path.get(j);
+			Patch<4> sec[TSC];
+			if (dirs.get(j)) {
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) patch_split_u(cur[k], &sec[k]);
+				const float um = (u0 + u1) * 0.5f;
+				if (second_half) u0 = um; else u1 = um;
+			} else {
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) patch_split_v(cur[k], &sec[k]);
+				const float vm = (v0 + v1) * 0.5f;
+				if (second_half) v0 = vm; else v1 = vm;
+			}
+			if (second_half) {
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) cur[k] = sec[k];
+			}
+		}
+	}
+	return found;
+}
+
 // ---------------------------------------------------------------------
 // Whole-scene traversal
 // ---------------------------------------------------------------------
@@ -419,7 +557,12 @@ struct Level {
 };
 
 // Traces one ray through the scene. Returns the device error flags.
-static __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
+// F is a mask of FEAT_* scene features; code for absent features is not
+// compiled into the variant, which keeps the flat-scene kernels small.
+template <unsigned F>
+__device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
+	constexpr bool NESTED = (F & FEAT_NESTED) != 0;
+	constexpr bool XFORM = (F & FEAT_XFORM) != 0;
 	unsigned err = 0;
 	float max_t = wr.occl ? 1.0f : INFINITY;
 	rec->obj = -1;
@@ -452,7 +595,7 @@ static __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, Hi
 	bool done = false;
 	while (!done) {
 		// leave finished levels, restoring the ray of the enclosing level
-		while (L > 0 && nsp == lv[L].stack_base) {
+		while (NESTED && L > 0 && nsp == lv[L].stack_base) {
 			const bool changed = lvl_frame[L] != lvl_frame[L - 1];
 			--L;
 			if (changed) {
@@ -531,14 +674,14 @@ static __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, Hi
 		const int shader = inst.shader >= 0 ? inst.shader : lv[L].shader;
 		const Frame& parent = lvl_frame[L] >= 0 ? frames[lvl_frame[L]] : none;
 
-		if (inst.kind == INST_ASSEMBLY) {
+		if (NESTED && inst.kind == INST_ASSEMBLY) {
 			if (L + 1 >= PSY_MAX_LEVELS) {
 				err |= ERRF_LEVELS;
 				continue;
 			}
 			const DevAssembly as = sc.assemblies[inst.data];
 			if (as.root == REF_EMPTY) continue;
-			if (inst.xform_count > 0) {
+			if (XFORM && inst.xform_count > 0) {
 				if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &frames[L + 1])) {
 					err |= ERRF_MOTION;
 					continue;
@@ -566,7 +709,7 @@ static __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, Hi
 
 		// object instance
 		LocalRay lr = r;
-		if (inst.xform_count > 0) {
+		if (XFORM && inst.xform_count > 0) {
 			Frame nf;
 			if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &nf)) {
 				err |= ERRF_MOTION;
@@ -595,16 +738,16 @@ static __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, Hi
 			}
 		} else if (ob.kind == OBJ_BILINEAR) {
 			const float* v = sc.fpool + ob.data;
-			if (ob.n0 == 1)
-				hit = patch_intersect<4, 1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
+				hit = bilinear_intersect<2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
 			else
-				hit = patch_intersect<4, 2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
-		} else if (ob.kind == OBJ_BICUBIC) {
+				hit = bilinear_intersect<1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+		} else if ((F & FEAT_BICUBIC) && ob.kind == OBJ_BICUBIC) {
 			const float* v = sc.fpool + ob.data;
-			if (ob.n0 == 1)
-				hit = patch_intersect<16, 1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
-			else
+			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
 				hit = patch_intersect<16, 2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+			else
+				hit = patch_intersect<16, 1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
 		}
 		if (hit) {
 			rec->obj = inst.data;
@@ -630,7 +773,9 @@ static __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, Hi
 // Transform from world space into the hit object's space at the ray time
 // (the Intersection::space of the reference), rebuilt from the hit path.
 // Returns false when the path carries no transform (identity).
-static __device__ bool hit_space(const DevScene& sc, const HitRec& rec, float time, M44* out, unsigned* err) {
+template <unsigned F>
+__device__ bool hit_space(const DevScene& sc, const HitRec& rec, float time, M44* out, unsigned* err) {
+	if (!(F & FEAT_XFORM)) return false;
 	Frame f;
 	f.count = 0;
 	for (int k = 0; k < rec.depth; ++k) {
