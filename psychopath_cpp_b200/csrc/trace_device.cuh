@@ -11,9 +11,8 @@
  * Per-ray state: the ray in the current instance space, a node stack,
  * a level stack for nested assemblies (element id prefix, inherited shader,
  * merged motion transforms, as the reference's xform_stack /
- * surface_shader_stack / element_id, tracer/tracer.cpp:125-219), and a
- * patch-split stack for the bisection of a patch (SPLIT_STACK_SIZE 64,
- * object/patch_utils.hpp:16).
+ * surface_shader_stack / element_id, tracer/tracer.cpp:125-219), and the
+ * path bits of the patch bisection (patch_intersect).
  */
 #ifndef PSY_TRACE_DEVICE_CUH
 #define PSY_TRACE_DEVICE_CUH
@@ -299,111 +298,60 @@ struct PatchHit {
 	float t, u, v, max_dim;
 };
 
-// Per-ray bisection of one patch with TSC time samples (TSC = 1 or 2):
-// intersect_rays_with_patch for a single ray (object/patch_utils.hpp:18-200).
-// The second half of every split is visited first, as in the reference.
-// Returns true when a new closest hit was recorded (or, for occlusion rays,
-// when any leaf was hit).
-template <int NV, int TSC>
-__device__ bool patch_intersect(const float* verts, float time, const LocalRay& r, float* max_t, bool occl,
-                                float dice_rate, float min_upoly, PatchHit* hit) {
-	struct Entry {
-		Patch<NV> q[TSC];
-		float u0, u1, v0, v1;
-	};
-	Entry stack[PSY_SPLIT_STACK];
-	int sp = 0;
-	Entry cur;
-#pragma unroll
-	for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur.q[k]);
-	cur.u0 = 0.0f; cur.u1 = 1.0f; cur.v0 = 0.0f; cur.v1 = 1.0f;
-	int t_index = 0;
-	float t_nalpha = 0.0f;
-	if (TSC > 1) {
-		const float t_time = time * (float)(TSC - 1);
-		t_index = (int)t_time;
-		t_nalpha = t_time - (float)t_index;
-		// time == 1.0 would index past the last sample (undefined in the
-		// reference); clamp to the last segment
-		if (t_index > TSC - 2) t_index = TSC - 2;
+// In-place halves of a split (Bilinear/Bicubic::split_u / split_v,
+// object/bilinear.hpp:59-82, object/bicubic.hpp:74-108): only the kept half
+// is written back, computed with the same operations as the full split.
+__device__ __forceinline__ void patch_half_u(Patch<4>& p, bool second) {
+	const V3 m01 = (p.p[0] + p.p[1]) * 0.5f;
+	const V3 m23 = (p.p[2] + p.p[3]) * 0.5f;
+	if (second) {
+		p.p[0] = m01;
+		p.p[2] = m23;
+	} else {
+		p.p[1] = m01;
+		p.p[3] = m23;
 	}
-	bool found = false;
-	int depth = 0;           // stack_i of the reference for `cur`
-	int depth_stack[PSY_SPLIT_STACK];
-	while (true) {
-		Box bb[TSC];
-		float max_dim = 0.0f;
-#pragma unroll
-		for (int k = 0; k < TSC; ++k) {
-			bb[k] = patch_bound<NV>(cur.q[k]);
-			const float ld = longest_axis(bb[k].hi - bb[k].lo);
-			max_dim = (k == 0) ? ld : smax(max_dim, ld);
-		}
-		float h0, h1;
-		bool h;
-		if (TSC == 1) h = box_hit(bb[0], r.o, r.dinv, *max_t, &h0, &h1);
-		else h = box_hit(box_lerp(t_nalpha, bb[t_index], bb[t_index + 1]), r.o, r.dinv, *max_t, &h0, &h1);
-		bool descend = false;
-		if (h) {
-			const float width = smax(ray_min_width(r.w, h0, h1) * dice_rate, min_upoly);
-			if (max_dim <= width || depth == PSY_SPLIT_STACK - 1) {
-				const float tt = (h0 + h1) * 0.5f;
-				if (tt > 0.0f && tt < *max_t) {
-					found = true;
-					if (occl) return true;
-					*max_t = tt;
-					hit->t = tt;
-					hit->u = (cur.u0 + cur.u1) * 0.5f;
-					hit->v = (cur.v0 + cur.v1) * 0.5f;
-					hit->max_dim = max_dim;
-				}
-			} else {
-				descend = true;
-			}
-		}
-		if (descend) {
-			// split: `cur` keeps the first half (pushed), the second half is next
-			Entry second;
-			const float ul = patch_ulen(cur.q[0]);
-			const float vl = patch_vlen(cur.q[0]);
-			if (ul > vl) {
-#pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_split_u(cur.q[k], &second.q[k]);
-				const float um = (cur.u0 + cur.u1) * 0.5f;
-				second.u0 = um; second.u1 = cur.u1; second.v0 = cur.v0; second.v1 = cur.v1;
-				cur.u1 = um;
-			} else {
-#pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_split_v(cur.q[k], &second.q[k]);
-				const float vm = (cur.v0 + cur.v1) * 0.5f;
-				second.u0 = cur.u0; second.u1 = cur.u1; second.v0 = vm; second.v1 = cur.v1;
-				cur.v1 = vm;
-			}
-			stack[sp] = cur;
-			depth_stack[sp] = depth;
-			++sp;
-			cur = second;
-			depth = depth + 1;
-		} else {
-			if (sp == 0) break;
-			--sp;
-			cur = stack[sp];
-			depth = depth_stack[sp];
-		}
+}
+__device__ __forceinline__ void patch_half_v(Patch<4>& p, bool second) {
+	const V3 m02 = (p.p[0] + p.p[2]) * 0.5f;
+	const V3 m13 = (p.p[1] + p.p[3]) * 0.5f;
+	if (second) {
+		p.p[0] = m02;
+		p.p[1] = m13;
+	} else {
+		p.p[2] = m02;
+		p.p[3] = m13;
 	}
-	return found;
+}
+// One de Casteljau split at 0.5 of four control points a,b,c,d (a row or a
+// column of a bicubic patch), keeping one half.
+__device__ __forceinline__ void bezier_half(V3& a, V3& b, V3& c, V3& d, bool second) {
+	const V3 tmp = (b + c) * 0.5f;
+	const V3 q2 = (d + c) * 0.5f;
+	const V3 q1 = (tmp + q2) * 0.5f;
+	const V3 a1 = (a + b) * 0.5f;
+	const V3 a2 = (tmp + a1) * 0.5f;
+	const V3 a3 = (a2 + q1) * 0.5f;
+	if (second) {
+		a = a3;
+		b = q1;
+		c = q2;
+	} else {
+		b = a1;
+		c = a2;
+		d = a3;
+	}
+}
+__device__ __forceinline__ void patch_half_u(Patch<16>& p, bool second) {
+#pragma unroll
+	for (int r = 0; r < 4; ++r) bezier_half(p.p[r * 4], p.p[r * 4 + 1], p.p[r * 4 + 2], p.p[r * 4 + 3], second);
+}
+__device__ __forceinline__ void patch_half_v(Patch<16>& p, bool second) {
+#pragma unroll
+	for (int c = 0; c < 4; ++c) bezier_half(p.p[c], p.p[c + 4], p.p[c + 8], p.p[c + 12], second);
 }
 
-// Bilinear patches: the same depth-first bisection without a stack of
-// sub-patches.  A node is identified by its path from the root (one bit per
-// split: 1 = second half, visited first) and the split direction taken at
-// each level; when a subtree is finished, the deepest pending first half is
-// rebuilt by replaying the recorded splits from the root.  Replaying runs
-// the same float operations in the same order as the original descent, so
-// every node's control points and uv range are bit-identical to the stored
-// ones, and the per-ray state stays in registers.  The reference's stack
-// index (its forced-leaf limit of 63) counts second halves only, which is
-// the population count of the path.
+// Path of a node in the bisection tree: one bit per split.
 struct Bits128 {
 	uint64_t lo, hi;
 	__device__ __forceinline__ bool get(int i) const { return i < 64 ? ((lo >> i) & 1ull) : ((hi >> (i - 64)) & 1ull); }
@@ -428,21 +376,35 @@ struct Bits128 {
 	__device__ __forceinline__ int popc() const { return __popcll(lo) + __popcll(hi); }
 };
 
-template <int TSC>
-__device__ bool bilinear_intersect(const float* verts, float time, const LocalRay& r, float* max_t, bool occl,
-                                   float dice_rate, float min_upoly, PatchHit* hit) {
-	Patch<4> root[TSC], cur[TSC];
+// Per-ray bisection of one patch with TSC time samples (TSC = 1 or 2):
+// intersect_rays_with_patch for a single ray (object/patch_utils.hpp:18-200).
+//
+// The reference walks the split tree depth first, second half before first
+// half, keeping the pending first halves on a stack.  Here a node is its
+// path from the root (1 = second half) plus the split directions; when a
+// subtree is finished the deepest pending first half is rebuilt by replaying
+// the recorded splits from the root patch.  The replay performs the same
+// float operations as the first descent, so every node's control points and
+// uv range are bit-identical to the stored ones, and the walk needs no
+// per-ray stack of sub-patches.  The reference's stack index (its forced
+// leaf at 63) counts second halves only: the population count of the path.
+//
+// Returns true when a new closest hit was recorded (or, for occlusion rays,
+// when any leaf was hit).
+template <int NV, int TSC>
+__device__ bool patch_intersect(const float* verts, float time, const LocalRay& r, float* max_t, bool occl,
+                                float dice_rate, float min_upoly, PatchHit* hit) {
+	Patch<NV> cur[TSC];
 #pragma unroll
-	for (int k = 0; k < TSC; ++k) {
-		patch_load<4>(verts + k * 12, &root[k]);
-		cur[k] = root[k];
-	}
+	for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur[k]);
 	int t_index = 0;
 	float t_nalpha = 0.0f;
 	if (TSC > 1) {
 		const float t_time = time * (float)(TSC - 1);
 		t_index = (int)t_time;
 		t_nalpha = t_time - (float)t_index;
+		// time == 1.0 would index past the last sample (undefined in the
+		// reference); clamp to the last segment
 		if (t_index > TSC - 2) t_index = TSC - 2;
 	}
 	Bits128 path{0, 0}, dirs{0, 0};  // dirs bit: 1 = split along u
@@ -454,14 +416,14 @@ __device__ bool bilinear_intersect(const float* verts, float time, const LocalRa
 		float max_dim = 0.0f;
 #pragma unroll
 		for (int k = 0; k < TSC; ++k) {
-			bb[k] = patch_bound<4>(cur[k]);
+			bb[k] = patch_bound<NV>(cur[k]);
 			const float ld = longest_axis(bb[k].hi - bb[k].lo);
 			max_dim = (k == 0) ? ld : smax(max_dim, ld);
 		}
 		float h0, h1;
 		bool h;
 		if (TSC == 1) h = box_hit(bb[0], r.o, r.dinv, *max_t, &h0, &h1);
-		else h = box_hit(box_lerp(t_nalpha, bb[t_index], bb[t_index + 1]), r.o, r.dinv, *max_t, &h0, &h1);
+		else h = box_hit(box_lerp(t_nalpha, bb[0], bb[TSC - 1]), r.o, r.dinv, *max_t, &h0, &h1);
 		bool descend = false;
 		if (h) {
 			const float width = smax(ray_min_width(r.w, h0, h1) * dice_rate, min_upoly);
@@ -481,19 +443,16 @@ __device__ bool bilinear_intersect(const float* verts, float time, const LocalRa
 			}
 		}
 		if (descend) {
-			Patch<4> second[TSC];
 			const bool along_u = patch_ulen(cur[0]) > patch_vlen(cur[0]);
 			if (along_u) {
 #pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_split_u(cur[k], &second[k]);
+				for (int k = 0; k < TSC; ++k) patch_half_u(cur[k], true);
 				u0 = (u0 + u1) * 0.5f;
 			} else {
 #pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_split_v(cur[k], &second[k]);
+				for (int k = 0; k < TSC; ++k) patch_half_v(cur[k], true);
 				v0 = (v0 + v1) * 0.5f;
 			}
-#pragma unroll
-			for (int k = 0; k < TSC; ++k) cur[k] = second[k];
 			path.set(depth, true);
 			dirs.set(depth, along_u);
 			++depth;
@@ -507,25 +466,20 @@ __device__ bool bilinear_intersect(const float* verts, float time, const LocalRa
 		path.truncate(depth);
 		dirs.truncate(depth);
 #pragma unroll
-		for (int k = 0; k < TSC; ++k) cur[k] = root[k];
+		for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur[k]);
 		u0 = 0.0f; u1 = 1.0f; v0 = 0.0f; v1 = 1.0f;
 		for (int j = 0; j < depth; ++j) {
 			const bool second_half = path.get(j);
-			Patch<4> sec[TSC];
 			if (dirs.get(j)) {
 #pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_split_u(cur[k], &sec[k]);
+				for (int k = 0; k < TSC; ++k) patch_half_u(cur[k], second_half);
 				const float um = (u0 + u1) * 0.5f;
 				if (second_half) u0 = um; else u1 = um;
 			} else {
 #pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_split_v(cur[k], &sec[k]);
+				for (int k = 0; k < TSC; ++k) patch_half_v(cur[k], second_half);
 				const float vm = (v0 + v1) * 0.5f;
 				if (second_half) v0 = vm; else v1 = vm;
-			}
-			if (second_half) {
-#pragma unroll
-				for (int k = 0; k < TSC; ++k) cur[k] = sec[k];
 			}
 		}
 	}
@@ -739,9 +693,9 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 		} else if (ob.kind == OBJ_BILINEAR) {
 			const float* v = sc.fpool + ob.data;
 			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-				hit = bilinear_intersect<2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_intersect<4, 2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
 			else
-				hit = bilinear_intersect<1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_intersect<4, 1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
 		} else if ((F & FEAT_BICUBIC) && ob.kind == OBJ_BICUBIC) {
 			const float* v = sc.fpool + ob.data;
 			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
