@@ -223,6 +223,29 @@ int psy_trace(psy_ctx* ctx, const psy_ray_soa* rays, uint32_t n, const psy_hit_s
  */
 int psy_trace_host(psy_ctx* ctx, const psy_ray_soa* rays, uint32_t n, const psy_hit_soa* hits);
 
+/*
+ * psy_trace_host without any allocation.  This entry point has no
+ * counterpart in the reference; it exists for callers that cannot let a
+ * trace call allocate device memory (a renderer whose pool allocator already
+ * holds all free device memory, or one whose other streams must not be
+ * stalled by the device-wide synchronisation cudaMalloc / cudaFree can
+ * cause).  The rays and hits are staged in one fixed-size device array
+ * compiled into the library (about 17 MB, reserved when the library's device
+ * code is loaded) instead of the context's growable scratch buffers.  Same
+ * arguments and results as psy_trace_host, on `stream` (NULL = default
+ * stream), synchronised before return.
+ *  - n > PSY_NOALLOC_MAX_RAYS fails with PSY_ERR_ARG before any device work.
+ *  - The array is one per device, shared by all contexts: calls that overlap
+ *    in time on one device race on it; serialise them.
+ *  - The first call on each device resolves the array's address; make it
+ *    before any stream capture begins on that device.
+ *  - No device or pinned memory is allocated; only a failing call may grow
+ *    the context's error message string.
+ */
+#define PSY_NOALLOC_MAX_RAYS 65536u
+int psy_trace_host_noalloc(psy_ctx* ctx, const psy_ray_soa* rays, uint32_t n, const psy_hit_soa* hits,
+                           void* stream);
+
 /* Waits for the context's work on `stream` and reports device-side errors. */
 int psy_sync(psy_ctx* ctx, void* stream);
 

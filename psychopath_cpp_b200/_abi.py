@@ -100,6 +100,7 @@ class RenderStats(C.Structure):
 # every symbol declared in include/psy_b200.h
 EXPORTED = ["psy_ctx_create", "psy_ctx_destroy", "psy_last_error", "psy_version", "psy_scene_upload",
             "psy_scene_stats_get", "psy_build_bvh4", "psy_build_light_tree", "psy_trace", "psy_trace_host", "psy_sync",
+            "psy_trace_host_noalloc",
             "psy_light_sample", "psy_render"]
 
 _lib = None
@@ -125,6 +126,9 @@ def load():
     L.psy_trace.argtypes = [C.c_void_p, C.POINTER(RaySoA), C.c_uint32, C.POINTER(HitSoA), C.c_void_p]
     L.psy_trace_host.argtypes = [C.c_void_p, C.POINTER(RaySoA), C.c_uint32, C.POINTER(HitSoA)]
     L.psy_sync.argtypes = [C.c_void_p, C.c_void_p]
+    if hasattr(L, "psy_trace_host_noalloc"):
+        L.psy_trace_host_noalloc.argtypes = [C.c_void_p, C.POINTER(RaySoA), C.c_uint32, C.POINTER(HitSoA),
+                                             C.c_void_p]
     if hasattr(L, "psy_light_sample"):
         L.psy_light_sample.argtypes = [C.c_void_p, C.POINTER(LightQuerySoA), C.c_uint32,
                                        C.POINTER(LightSampleSoA), C.c_void_p]

@@ -265,6 +265,21 @@ class Tracer:
         self.ctx.check(self.ctx.L.psy_trace_host(self.ctx.h, C.byref(rs), n, C.byref(hs)))
         return out
 
+    def trace_noalloc(self, rays: dict, fields=("hit", "id", "t", "uv"), stream=None) -> Dict[str, np.ndarray]:
+        """psy_trace_host_noalloc: as trace(), staged in the library's
+        fixed-size device array (at most NOALLOC_MAX_RAYS rays per call)."""
+        n = len(rays["time"])
+        rs, keep = _ray_soa_host(rays)
+        out = {}
+        hs = _abi.HitSoA()
+        for f in fields:
+            dt, w = HIT_FIELDS[f]
+            arr = np.zeros((n, w) if w > 1 else (n,), dt)
+            out[f] = arr
+            setattr(hs, f, arr.ctypes.data_as(C.c_void_p))
+        self.ctx.check(self.ctx.L.psy_trace_host_noalloc(self.ctx.h, C.byref(rs), n, C.byref(hs), stream))
+        return out
+
     def trace_device(self, rays: dict, hits: dict, stream=None) -> None:
         """Device form (psy_trace): `rays` and `hits` map field names to
         CUDA tensors (anything with .data_ptr()); stream-ordered."""
