@@ -47,7 +47,6 @@ struct RenderParams {
 // Path state of one wave, structure of arrays (PTState,
 // integrator/path_trace_integrator.hpp:49-63).
 struct PathSoA {
-	uint32_t* pix;      // x | y << 16
 	uint32_t* smp;      // sampler offset
 	uint32_t* dimstep;  // next sampler dimension | step << 16
 	float* wl;
@@ -55,16 +54,25 @@ struct PathSoA {
 	float* last_pdf;
 	float4* col;
 	float4* fcol;
-	float4* lcol;
+	float4* lcol;       // between the shadow ray and its result: the light's contribution
 	float* hit;         // stored intersection, 16 floats per path
 	float* pray;        // previous ray, 16 floats per path
 	float* sample;      // film sample XYZ, 3 floats per path
 };
 
+// Rays and hits of a wave by queue position (cap = the wave's path capacity).
+struct WaveBufs {
+	float4* ray[2];     // [0] camera / bounce rays, [1] shadow rays: 5 planes of cap float4
+	float4* hit_f;      // t, u, v, max_dim
+	int4* hit_i;        // 3 planes: obj, kind | depth << 8, shader, path[0]; path[1..4]; path[5..7]
+	uint8_t* occl;      // shadow ray result: 1 = blocked (or no shadow ray)
+	int cap;
+};
+
 struct WaveQueues {
 	int* q0;
 	int* q1;
-	int* counters;      // per step: live count out, work counter
+	int* counters;      // render_counter_count(path_length) work and live counters
 	unsigned long long* rays;
 };
 
@@ -76,11 +84,10 @@ struct LightSampleSoADev {
 	uint64_t* id;
 };
 
-// Persistent grid size for the wavefront step kernels (resident blocks x SMs).
-int render_grid(unsigned features);
+int render_counter_count(uint32_t path_length);
 cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
-                               const WaveQueues& wq, float* xyz, uint32_t* counts, unsigned* status, int grid,
-                               cudaStream_t st, uint32_t* launches);
+                               const WaveBufs& wb, const WaveQueues& wq, float* xyz, uint32_t* counts,
+                               unsigned* status, cudaStream_t st, uint32_t* launches);
 cudaError_t launch_light_sample(const DevScene& sc, const LightQuerySoADev& q, const LightSampleSoADev& o, uint32_t n,
                                 float ident_inv, unsigned* status, cudaStream_t st);
 

@@ -450,7 +450,6 @@ int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* 
 	int rc;
 	auto buf = [&](const char* name, size_t bytes) -> void* { return ctx->scratch_buffer(name, bytes, &rc); };
 	PathSoA ps;
-	ps.pix = (uint32_t*)buf("r_pix", P * 4);
 	ps.smp = (uint32_t*)buf("r_smp", P * 4);
 	ps.dimstep = (uint32_t*)buf("r_dimstep", P * 4);
 	ps.wl = (float*)buf("r_wl", P * 4);
@@ -465,9 +464,17 @@ int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* 
 	WaveQueues wq;
 	wq.q0 = (int*)buf("r_q0", P * 4);
 	wq.q1 = (int*)buf("r_q1", P * 4);
-	wq.counters = (int*)buf("r_counters", sizeof(int) * 2 * (path_length * 2 + 1));
+	wq.counters = (int*)buf("r_counters", sizeof(int) * render_counter_count(path_length));
 	wq.rays = (unsigned long long*)buf("r_rays", sizeof(unsigned long long));
-	if (!ps.pix || !ps.smp || !ps.dimstep || !ps.wl || !ps.time || !ps.last_pdf || !ps.col || !ps.fcol || !ps.lcol ||
+	WaveBufs wb;
+	wb.cap = (int)P;
+	wb.ray[0] = (float4*)buf("r_ray0", P * 80);
+	wb.ray[1] = (float4*)buf("r_ray1", P * 80);
+	wb.hit_f = (float4*)buf("r_hitf", P * 16);
+	wb.hit_i = (int4*)buf("r_hiti", P * 48);
+	wb.occl = (uint8_t*)buf("r_occl", P);
+	if (!wb.ray[0] || !wb.ray[1] || !wb.hit_f || !wb.hit_i || !wb.occl) return rc ? rc : PSY_ERR_OOM;
+	if (!ps.smp || !ps.dimstep || !ps.wl || !ps.time || !ps.last_pdf || !ps.col || !ps.fcol || !ps.lcol ||
 	    !ps.hit || !ps.pray || !ps.sample || !wq.q0 || !wq.q1 || !wq.counters || !wq.rays)
 		return rc ? rc : PSY_ERR_OOM;
 	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(wq.rays, 0, sizeof(unsigned long long), st), "memset"))) return rc;
@@ -484,13 +491,12 @@ int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* 
 	rp.min_y = -rp.max_y;
 	rp.ident_inv = ctx->ident_inv;
 	uint32_t launches = 0, waves = 0;
-	const int grid = render_grid(ctx->dev.features);
 	for (uint64_t base = 0; base < total; base += P) {
 		rp.wave_base = base;
 		rp.wave_paths = (int)((total - base) < P ? (total - base) : P);
 		if ((rc = ctx_cuda(ctx,
-		                   launch_render_wave(ctx->dev, ctx->halton, rp, ps, wq, xyz, counts, ctx->d_status, grid,
-		                                      st, &launches),
+		                   launch_render_wave(ctx->dev, ctx->halton, rp, ps, wb, wq, xyz, counts, ctx->d_status, st,
+		                                      &launches),
 		                   "render launch")))
 			return rc;
 		++waves;

@@ -38,8 +38,17 @@ enum : unsigned {
 	FEAT_BICUBIC = 4u,       // bicubic patches
 	FEAT_PATCH_MOTION = 8u,  // patches with two time samples
 	FEAT_FLAT = 0u,
+	FEAT_STILL = 7u,         // everything but patch motion
 	FEAT_ALL = 15u
 };
+
+// The compiled variant (FEAT_FLAT, FEAT_STILL or FEAT_ALL) that covers a
+// scene's features.
+inline unsigned feature_variant(unsigned f) {
+	if (f == FEAT_FLAT) return FEAT_FLAT;
+	if ((f & ~FEAT_STILL) == 0u) return FEAT_STILL;
+	return FEAT_ALL;
+}
 
 // A child reference in a BVH4 node or an assembly root:
 //   >= 0          inner node index (global)

@@ -4,11 +4,23 @@
  *
  * The reference renders a bucket as a stream of paths and loops
  *   generate one ray per live path -> Tracer::trace -> update -> partition.
- * Here a wave of paths lives in HBM as SoA state; each step of the loop is
- * one persistent kernel over the wave's live-path queue that generates the
- * path's ray (camera / shadow / bounce), traces it, updates the path, and
- * appends still-live paths to the next queue with one atomic per warp
- * (ballot + popc compaction).  Finished paths write their film sample
+ * Here a wave of paths lives in HBM as SoA state and the loop is split into
+ * kernels that each do one kind of work, so the traversal kernels carry no
+ * shading state and the shading kernels no traversal state:
+ *
+ *   camera_gen            camera rays of every path of the wave
+ *   trace<closest>        Tracer::trace of the ray buffer (closest hits)
+ *   shade_hit             update_path after a camera / bounce ray, then
+ *                         next_ray_for_path's shadow step: light-tree sample
+ *                         and shadow ray; live paths are compacted into the
+ *                         next queue (ballot + popc, one atomic per warp)
+ *   trace<occlusion>      Tracer::trace of the shadow rays
+ *   shade_shadow          update_path after the shadow ray, then the bounce
+ *                         ray (the path stays at its queue position)
+ *   ... trace<closest> -> shade_hit -> ... for path_length bounces.
+ *
+ * Rays and hits are stored by queue position (coalesced), path state by
+ * path slot.  Finished paths write their film sample
  * (Color_XYZ(col) * XYZ_NORM_FAC); a per-wave reduction adds each pixel's
  * samples in sample order.
  */
@@ -17,13 +29,71 @@
 
 namespace psy {
 
-enum : int { STEP_CAMERA = 0, STEP_SHADOW = 1, STEP_BOUNCE = 2 };
-
 __device__ __forceinline__ float4 f4(const Spec& s) { return make_float4(s.e[0], s.e[1], s.e[2], s.e[3]); }
 __device__ __forceinline__ Spec sp(float4 v) {
 	Spec s;
 	s.e[0] = v.x; s.e[1] = v.y; s.e[2] = v.z; s.e[3] = v.w;
 	return s;
+}
+
+// ---------------------------------------------------------------------
+// Ray and hit records by queue position
+// ---------------------------------------------------------------------
+// Ray planes (5 x float4 per position):
+//   0: o.xyz, time   1: d.xyz, odx.x   2: odx.yz, ody.xy   3: ody.z, ddx.xyz
+//   4: ddy.xyz, flag (1 = no ray: the shadow step found no light sample)
+__device__ __forceinline__ void store_ray(float4* rb, int cap, int i, const WorldRayD& r, float flag) {
+	rb[i] = make_float4(r.o.x, r.o.y, r.o.z, r.time);
+	rb[cap + i] = make_float4(r.d.x, r.d.y, r.d.z, r.odx.x);
+	rb[2 * cap + i] = make_float4(r.odx.y, r.odx.z, r.ody.x, r.ody.y);
+	rb[3 * cap + i] = make_float4(r.ody.z, r.ddx.x, r.ddx.y, r.ddx.z);
+	rb[4 * cap + i] = make_float4(r.ddy.x, r.ddy.y, r.ddy.z, flag);
+}
+__device__ __forceinline__ float load_ray(const float4* rb, int cap, int i, WorldRayD* r) {
+	const float4 a = rb[i], b = rb[cap + i], c = rb[2 * cap + i], d = rb[3 * cap + i], e = rb[4 * cap + i];
+	r->o = V3(a.x, a.y, a.z);
+	r->time = a.w;
+	r->d = V3(b.x, b.y, b.z);
+	r->odx = V3(b.w, c.x, c.y);
+	r->ody = V3(c.z, c.w, d.x);
+	r->ddx = V3(d.y, d.z, d.w);
+	r->ddy = V3(e.x, e.y, e.z);
+	return e.w;
+}
+
+// Hit planes: 0: t, u, v, max_dim (float4)   1: obj, kind | depth << 8,
+// shader, path[0]   2: path[1..4]   3: path[5..7] (int4).  The path planes
+// beyond the hit's depth are neither written nor read.
+__device__ __forceinline__ void store_rec(const WaveBufs& wb, int i, const HitRec& h) {
+	wb.hit_f[i] = make_float4(h.t, h.u, h.v, h.max_dim);
+	const int cap = wb.cap;
+	if (h.obj < 0) {
+		wb.hit_i[i] = make_int4(-1, 0, -1, 0);
+		return;
+	}
+	wb.hit_i[i] = make_int4(h.obj, h.kind | (h.depth << 8), h.shader, h.path[0]);
+	if (h.depth > 1) wb.hit_i[cap + i] = make_int4(h.path[1], h.path[2], h.path[3], h.path[4]);
+	if (h.depth > 5) wb.hit_i[2 * cap + i] = make_int4(h.path[5], h.path[6], h.path[7], 0);
+}
+__device__ __forceinline__ void load_rec(const WaveBufs& wb, int i, HitRec* h) {
+	const float4 f = wb.hit_f[i];
+	h->t = f.x; h->u = f.y; h->v = f.z; h->max_dim = f.w;
+	const int4 a = wb.hit_i[i];
+	h->obj = a.x;
+	h->kind = a.y & 0xff;
+	h->depth = a.y >> 8;
+	h->shader = a.z;
+	h->path[0] = a.w;
+	h->id = 0;
+	const int cap = wb.cap;
+	if (h->depth > 1) {
+		const int4 b = wb.hit_i[cap + i];
+		h->path[1] = b.x; h->path[2] = b.y; h->path[3] = b.z; h->path[4] = b.w;
+	}
+	if (h->depth > 5) {
+		const int4 c = wb.hit_i[2 * cap + i];
+		h->path[5] = c.x; h->path[6] = c.y; h->path[7] = c.z;
+	}
 }
 
 // World-space shading data of the stored intersection (the PTState::inter
@@ -124,8 +194,7 @@ __device__ __forceinline__ void propagate_differentials(const StoredHit& h, Worl
 	out->ddy = (y * 0.15f) / len;
 }
 
-__device__ __forceinline__ void finish_path(const RenderParams& rp, const PathSoA& ps, int slot, const Spec& col,
-                                            float wl) {
+__device__ __forceinline__ void finish_path(const PathSoA& ps, int slot, const Spec& col, float wl) {
 	float xyz[3];
 	spec_to_xyz(col, wl, xyz);
 	float3 o;
@@ -135,97 +204,150 @@ __device__ __forceinline__ void finish_path(const RenderParams& rp, const PathSo
 	reinterpret_cast<float3*>(ps.sample)[slot] = o;
 }
 
-template <int KIND, unsigned F>
-__global__ void __launch_bounds__(128) step_kernel(DevScene sc, HaltonDev hd, RenderParams rp, PathSoA ps,
-                                                  const int* __restrict__ q_in, const int* n_in, int* q_out,
-                                                  int* n_out, int* work, unsigned long long* ray_count,
-                                                  unsigned* status) {
-	const int lane = threadIdx.x & 31;
-	const int n = (KIND == STEP_CAMERA) ? rp.wave_paths : *n_in;
+// Warp-wide work fetch: lane 0 takes the next 32 queue positions.
+__device__ __forceinline__ int fetch32(int* work) {
+	int base = 0;
+	if ((threadIdx.x & 31) == 0) base = atomicAdd(work, 32);
+	return __shfl_sync(0xffffffffu, base, 0);
+}
+
+// ---------------------------------------------------------------------
+// Camera rays (next_ray_for_path, step 0: path_trace_integrator.cpp:109-125)
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(128) camera_gen_kernel(DevScene sc, HaltonDev hd, RenderParams rp, PathSoA ps,
+                                                         WaveBufs wb) {
+	const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+	if (slot >= rp.wave_paths) return;
+	const uint64_t gidx = rp.wave_base + (uint64_t)slot;
+	const uint64_t pixel = gidx / rp.spp;
+	const uint32_t px = (uint32_t)(pixel % rp.width);
+	const uint32_t py = (uint32_t)(pixel / rp.width);
+	const uint32_t s = (uint32_t)(gidx % rp.spp);
+	const uint32_t smp = sampler_offset(px, py, s, rp.seed);
+	uint32_t dim = 0;
+	const float wl = (sampler_get(hd, smp, dim++) * (WAVELENGTH_MAX - WAVELENGTH_MIN)) + WAVELENGTH_MIN;
+	const float samp_x = (fast_logit(sampler_get(hd, smp, dim++), 1.5f) + 0.5f + (float)px) / (float)rp.width;
+	const float samp_y = (fast_logit(sampler_get(hd, smp, dim++), 1.5f) + 0.5f + (float)py) / (float)rp.height;
+	const float rx = (float)(((double)samp_x - 0.5) * (double)(rp.max_x - rp.min_x));
+	const float ry = (float)((0.5 - (double)samp_y) * (double)(rp.max_y - rp.min_y));
+	const float dx = (rp.max_x - rp.min_x) / (float)rp.width;
+	const float dy = (rp.max_y - rp.min_y) / (float)rp.height;
+	const float samp_a = sampler_get(hd, smp, dim++);
+	const float samp_b = sampler_get(hd, smp, dim++);
+	const float samp_c = sampler_get(hd, smp, dim++);
+	WorldRayD wr;
+	camera_ray(sc, rx, ry, dx, dy, samp_c, samp_a, samp_b, &wr);
+	store_ray(wb.ray[0], wb.cap, slot, wr, 0.0f);
+	ps.smp[slot] = smp;
+	ps.dimstep[slot] = dim;  // step 0
+	ps.wl[slot] = wl;
+	ps.time[slot] = wr.time;
+	ps.last_pdf[slot] = 0.0f;
+	ps.col[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	ps.fcol[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+}
+
+// ---------------------------------------------------------------------
+// Traversal of a ray buffer (Tracer::trace, tracer/tracer.cpp:38-121)
+// ---------------------------------------------------------------------
+// n_dev == nullptr: n_host rays.  OCCL: occlusion rays, the result (1 =
+// blocked or no ray) goes to wb.occl by position.
+template <unsigned F, bool OCCL>
+__global__ void __launch_bounds__(128) trace_wave_kernel(DevScene sc, WaveBufs wb, const float4* __restrict__ rb,
+                                                         const int* n_dev, int n_host, int* work,
+                                                         unsigned long long* ray_count, unsigned* status) {
+	const int n = n_dev ? *n_dev : n_host;
 	unsigned err = 0;
 	unsigned long long rays = 0;
 	while (true) {
-		int base;
-		if (lane == 0) base = atomicAdd(work, 32);
-		base = __shfl_sync(0xffffffffu, base, 0);
+		const int base = fetch32(work);
+		if (base >= n) break;
+		const int i = base + (threadIdx.x & 31);
+		if (i < n) {
+			WorldRayD wr;
+			const float flag = load_ray(rb, wb.cap, i, &wr);
+			wr.occl = OCCL;
+			if (OCCL && flag != 0.0f) {
+				wb.occl[i] = 1;
+			} else {
+				HitRec rec;
+				err |= trace_ray<F>(sc, wr, &rec);
+				++rays;
+				if (OCCL) wb.occl[i] = rec.obj >= 0 ? 1 : 0;
+				else store_rec(wb, i, rec);
+			}
+		}
+	}
+	for (int o = 16; o > 0; o >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, o);
+	if ((threadIdx.x & 31) == 0 && rays) atomicAdd(ray_count, rays);
+	if (err) atomicOr(status, err);
+}
+
+// ---------------------------------------------------------------------
+// After a camera (CAMERA) or bounce ray: update_path
+// (path_trace_integrator.cpp:251-272 and 273-302), then the shadow step of
+// next_ray_for_path (path_trace_integrator.cpp:126-184).
+// ---------------------------------------------------------------------
+template <bool CAMERA, unsigned F>
+__global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev hd, RenderParams rp, PathSoA ps,
+                                                        WaveBufs wb, const int* __restrict__ q_in, const int* n_dev,
+                                                        int n_host, int* q_out, int* n_out, int* work,
+                                                        unsigned* status) {
+	const int lane = threadIdx.x & 31;
+	const int n = n_dev ? *n_dev : n_host;
+	unsigned err = 0;
+	while (true) {
+		const int base = fetch32(work);
 		if (base >= n) break;
 		const int i = base + lane;
 		bool live = false;
 		int slot = -1;
+		WorldRayD sray;
+		float sflag = 1.0f;
 		if (i < n) {
-			slot = (KIND == STEP_CAMERA) ? i : q_in[i];
-			// ---- load path state
-			uint32_t smp, dim, step;
-			float wl, time, last_pdf;
-			Spec col, fcol, lcol;
-			const uint32_t pix = ps.pix[slot];
-			const uint32_t px = pix & 0xffffu, py = pix >> 16;
-			if (KIND == STEP_CAMERA) {
-				const uint64_t gidx = rp.wave_base + (uint64_t)slot;
-				const uint32_t s = (uint32_t)(gidx % rp.spp);
-				smp = sampler_offset(px, py, s, rp.seed);
-				dim = 0;
-				step = 0;
-				wl = (sampler_get(hd, smp, dim++) * (WAVELENGTH_MAX - WAVELENGTH_MIN)) + WAVELENGTH_MIN;
-				time = 0.0f;
-				last_pdf = 0.0f;
-				for (int k = 0; k < 4; ++k) {
-					col.e[k] = 0.0f;
-					fcol.e[k] = 1.0f;
-					lcol.e[k] = 0.0f;
+			slot = q_in ? q_in[i] : i;
+			const uint32_t smp = ps.smp[slot];
+			const uint32_t ds = ps.dimstep[slot];
+			uint32_t dim = ds & 0xffffu;
+			uint32_t step = ds >> 16;
+			const float wl = ps.wl[slot];
+			const float time = ps.time[slot];
+			const float last_pdf = ps.last_pdf[slot];
+			Spec col = sp(ps.col[slot]);
+			const Spec fcol = sp(ps.fcol[slot]);
+			WorldRayD wr;
+			load_ray(wb.ray[0], wb.cap, i, &wr);
+			HitRec rec;
+			load_rec(wb, i, &rec);
+			bool done = false;
+			StoredHit sh;
+			if (rec.obj >= 0) {
+				int closure;
+				float ecol[3], lpdf;
+				make_stored<F>(sc, rec, wr, rp.ident_inv, &sh, &closure, ecol, &lpdf, &err);
+				if (closure == CLOSURE_EMIT) {
+					done = true;
+					const Spec e = rgb_to_spec(ecol, wl);
+					if (!CAMERA && last_pdf != 0.0f) {
+						const float mis_inv_pdf = power_heuristic(last_pdf, lpdf) / last_pdf;
+						for (int k = 0; k < 4; ++k) col.e[k] += ((fcol.e[k] * last_pdf) * e.e[k]) * mis_inv_pdf;
+					} else {
+						for (int k = 0; k < 4; ++k) col.e[k] += fcol.e[k] * e.e[k];
+					}
+				} else if (closure != CLOSURE_LAMBERT) {
+					done = true;  // closures outside the supported set end the path
 				}
 			} else {
-				smp = ps.smp[slot];
-				const uint32_t ds = ps.dimstep[slot];
-				dim = ds & 0xffffu;
-				step = ds >> 16;
-				wl = ps.wl[slot];
-				time = ps.time[slot];
-				last_pdf = ps.last_pdf[slot];
-				col = sp(ps.col[slot]);
-				fcol = sp(ps.fcol[slot]);
-				lcol = sp(ps.lcol[slot]);
+				done = true;
+				const Spec bg = rgb_to_spec(sc.background, wl);
+				for (int k = 0; k < 4; ++k) col.e[k] += fcol.e[k] * bg.e[k];
 			}
-			StoredHit sh;
-			if (KIND != STEP_CAMERA) load_hit(ps, slot, &sh);
-			bool done = false;
-
-			if (KIND == STEP_CAMERA) {
-				// next_ray_for_path, step 0 (path_trace_integrator.cpp:109-125)
-				const float samp_x = (fast_logit(sampler_get(hd, smp, dim++), 1.5f) + 0.5f + (float)px) / (float)rp.width;
-				const float samp_y = (fast_logit(sampler_get(hd, smp, dim++), 1.5f) + 0.5f + (float)py) / (float)rp.height;
-				const float rx = (float)(((double)samp_x - 0.5) * (double)(rp.max_x - rp.min_x));
-				const float ry = (float)((0.5 - (double)samp_y) * (double)(rp.max_y - rp.min_y));
-				const float dx = (rp.max_x - rp.min_x) / (float)rp.width;
-				const float dy = (rp.max_y - rp.min_y) / (float)rp.height;
-				const float samp_a = sampler_get(hd, smp, dim++);
-				const float samp_b = sampler_get(hd, smp, dim++);
-				const float samp_c = sampler_get(hd, smp, dim++);
-				WorldRayD wr;
-				camera_ray(sc, rx, ry, dx, dy, samp_c, samp_a, samp_b, &wr);
-				time = wr.time;
-				HitRec rec;
-				err |= trace_ray<F>(sc, wr, &rec);
-				++rays;
-				// update_path for a camera ray (path_trace_integrator.cpp:251-272)
-				if (rec.obj >= 0) {
-					int closure;
-					float ecol[3], lpdf;
-					make_stored<F>(sc, rec, wr, rp.ident_inv, &sh, &closure, ecol, &lpdf, &err);
-					if (closure == CLOSURE_EMIT) {
-						done = true;
-						const Spec e = rgb_to_spec(ecol, wl);
-						for (int k = 0; k < 4; ++k) col.e[k] += fcol.e[k] * e.e[k];
-					} else if (closure != CLOSURE_LAMBERT) {
-						done = true;  // closures outside the supported set end the path
-					}
-				} else {
-					done = true;
-					const Spec bg = rgb_to_spec(sc.background, wl);
-					for (int k = 0; k < 4; ++k) col.e[k] += fcol.e[k] * bg.e[k];
-				}
-			} else if (KIND == STEP_SHADOW) {
-				// next_ray_for_path, shadow step (path_trace_integrator.cpp:126-184)
+			step++;
+			if (step == rp.path_length * 2) done = true;
+			if (done) {
+				finish_path(ps, slot, col, wl);
+			} else {
+				// shadow step: light-tree sample and shadow ray
 				LightQuery q;
 				q.n = sampler_get(hd, smp, dim++);
 				q.u = sampler_get(hd, smp, dim++);
@@ -241,94 +363,34 @@ __global__ void __launch_bounds__(128) step_kernel(DevScene sc, HaltonDev hd, Re
 				q.selection_pdf = 1.0f;
 				q.light_sample_pdf = 1.0f;
 				light_tree_sample(sc, &q, rp.ident_inv);
+				float4 contrib = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 				if (q.valid) {
 					const float bsdf_pdf = lambert_pdf(sh.d, q.to_light, sh.n);
 					const float mis_inv_pdf = power_heuristic(q.light_sample_pdf, bsdf_pdf) / q.light_sample_pdf;
 					const float lc = (float)rp.light_count;
+					Spec lcol;
 					for (int k = 0; k < 4; ++k) lcol.e[k] = ((q.spec.e[k] * mis_inv_pdf) * lc) / q.selection_pdf;
-					WorldRayD wr;
-					wr.o = sh.p + sh.off;
-					wr.d = (q.to_light - sh.off) * 0.9995f;
-					wr.time = time;
-					wr.occl = true;
-					propagate_differentials(sh, &wr);
-					HitRec rec;
-					err |= trace_ray<F>(sc, wr, &rec);
-					++rays;
-					// update_path, shadow result (path_trace_integrator.cpp:235-249)
-					if (rec.obj < 0) {
-						const Spec fac = lambert_eval(sh.col, sh.d, wr.d, sh.n, wl);
-						for (int k = 0; k < 4; ++k) col.e[k] += (fcol.e[k] * lcol.e[k]) * fac.e[k];
-					}
+					sray.o = sh.p + sh.off;
+					sray.d = (q.to_light - sh.off) * 0.9995f;
+					sray.time = time;
+					sray.occl = true;
+					propagate_differentials(sh, &sray);
+					// the light's contribution if the shadow ray is not blocked
+					// (update_path, shadow result: path_trace_integrator.cpp:235-249)
+					const Spec fac = lambert_eval(sh.col, sh.d, sray.d, sh.n, wl);
+					Spec c;
+					for (int k = 0; k < 4; ++k) c.e[k] = (fcol.e[k] * lcol.e[k]) * fac.e[k];
+					contrib = f4(c);
+					sflag = 0.0f;
 				} else {
 					err |= ERRF_NOLIGHT;
+					sray.o = V3(0.0f); sray.d = V3(0.0f, 0.0f, 1.0f); sray.time = time;
+					sray.odx = sray.ody = sray.ddx = sray.ddy = V3(0.0f);
 				}
-			} else {
-				// next_ray_for_path, bounce step (path_trace_integrator.cpp:185-223).  The
-				// reference passes two sampler.next() calls as arguments; g++ evaluates
-				// them right to left, so the second draw is `si` and the first `sj`.
-				const float sj = sampler_get(hd, smp, dim++);
-				const float si = sampler_get(hd, smp, dim++);
-				V3 nn = normalized(sh.n);
-				if (dot(nn, sh.d) > 0.0f) nn = nn * -1.0f;
-				const V3 dir = cosine_sample_hemisphere(si, sj);
-				float pdf = dir.z * (float)PSY_INV_PI_D;
-				const V3 out = zup_to_vec(dir, nn);
-				const Spec filter = lambert_eval(sh.col, sh.d, out, sh.n, wl);
-				WorldRayD wr;
-				wr.o = sh.p + sh.off;
-				wr.d = out;
-				wr.time = time;
-				wr.occl = false;
-				propagate_differentials(sh, &wr);
-				if (pdf < 0.00001f) pdf = 0.00001f;
-				for (int k = 0; k < 4; ++k) fcol.e[k] *= filter.e[k] / pdf;
-				last_pdf = pdf;
-				HitRec rec;
-				err |= trace_ray<F>(sc, wr, &rec);
-				++rays;
-				if (rec.obj >= 0) {
-					int closure;
-					float ecol[3], lpdf;
-					StoredHit nh;
-					make_stored<F>(sc, rec, wr, rp.ident_inv, &nh, &closure, ecol, &lpdf, &err);
-					if (closure == CLOSURE_EMIT) {
-						done = true;
-						const Spec e = rgb_to_spec(ecol, wl);
-						if (last_pdf != 0.0f) {
-							const float mis_inv_pdf = power_heuristic(last_pdf, lpdf) / last_pdf;
-							for (int k = 0; k < 4; ++k) col.e[k] += ((fcol.e[k] * last_pdf) * e.e[k]) * mis_inv_pdf;
-						} else {
-							for (int k = 0; k < 4; ++k) col.e[k] += fcol.e[k] * e.e[k];
-						}
-					} else if (closure == CLOSURE_LAMBERT) {
-						sh = nh;
-					} else {
-						done = true;
-					}
-				} else {
-					done = true;
-					const Spec bg = rgb_to_spec(sc.background, wl);
-					for (int k = 0; k < 4; ++k) col.e[k] += fcol.e[k] * bg.e[k];
-				}
-			}
-			step++;
-			if (step == rp.path_length * 2) done = true;
-
-			if (done) {
-				finish_path(rp, ps, slot, col, wl);
-			} else {
-				ps.smp[slot] = smp;
 				ps.dimstep[slot] = (dim & 0xffffu) | (step << 16);
-				ps.wl[slot] = wl;
-				ps.time[slot] = time;
-				ps.last_pdf[slot] = last_pdf;
 				ps.col[slot] = f4(col);
-				ps.fcol[slot] = f4(fcol);
-				ps.lcol[slot] = f4(lcol);
-				if (KIND != STEP_SHADOW) {
-					store_hit(ps, slot, sh);
-				}
+				ps.lcol[slot] = contrib;
+				store_hit(ps, slot, sh);
 				live = true;
 			}
 		}
@@ -337,24 +399,72 @@ __global__ void __launch_bounds__(128) step_kernel(DevScene sc, HaltonDev hd, Re
 		int out_base = 0;
 		if (lane == 0 && m) out_base = atomicAdd(n_out, __popc(m));
 		out_base = __shfl_sync(0xffffffffu, out_base, 0);
-		if (live) q_out[out_base + __popc(m & ((1u << lane) - 1u))] = slot;
+		if (live) {
+			const int j = out_base + __popc(m & ((1u << lane) - 1u));
+			q_out[j] = slot;
+			store_ray(wb.ray[1], wb.cap, j, sray, sflag);
+		}
 	}
-	// warp-aggregated ray count
-	for (int o = 16; o > 0; o >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, o);
-	if (lane == 0 && rays) atomicAdd(ray_count, rays);
 	if (err) atomicOr(status, err);
 }
 
-// Pixel coordinates of every path slot of a wave (paths are ordered pixel
-// by pixel, samples innermost).
-__global__ void pix_init_kernel(RenderParams rp, PathSoA ps) {
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= rp.wave_paths) return;
-	const uint64_t gidx = rp.wave_base + (uint64_t)i;
-	const uint64_t pixel = gidx / rp.spp;
-	const uint32_t x = (uint32_t)(pixel % rp.width);
-	const uint32_t y = (uint32_t)(pixel / rp.width);
-	ps.pix[i] = x | (y << 16);
+// ---------------------------------------------------------------------
+// After the shadow ray: update_path (path_trace_integrator.cpp:235-249),
+// then the bounce step of next_ray_for_path (path_trace_integrator.cpp:185-223).
+// Paths keep their queue position.
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(128) shade_shadow_kernel(HaltonDev hd, RenderParams rp, PathSoA ps, WaveBufs wb,
+                                                           const int* __restrict__ q_in, const int* n_dev, int* work) {
+	const int n = *n_dev;
+	while (true) {
+		const int base = fetch32(work);
+		if (base >= n) break;
+		const int i = base + (threadIdx.x & 31);
+		if (i >= n) continue;
+		const int slot = q_in[i];
+		const uint32_t smp = ps.smp[slot];
+		const uint32_t ds = ps.dimstep[slot];
+		uint32_t dim = ds & 0xffffu;
+		uint32_t step = ds >> 16;
+		const float wl = ps.wl[slot];
+		Spec col = sp(ps.col[slot]);
+		if (wb.occl[i] == 0) {
+			const Spec c = sp(ps.lcol[slot]);
+			for (int k = 0; k < 4; ++k) col.e[k] += c.e[k];
+		}
+		step++;
+		if (step == rp.path_length * 2) {
+			finish_path(ps, slot, col, wl);
+			continue;
+		}
+		StoredHit sh;
+		load_hit(ps, slot, &sh);
+		Spec fcol = sp(ps.fcol[slot]);
+		// The reference passes two sampler.next() calls as arguments; g++
+		// evaluates them right to left, so the second draw is `si` and the
+		// first `sj`.
+		const float sj = sampler_get(hd, smp, dim++);
+		const float si = sampler_get(hd, smp, dim++);
+		V3 nn = normalized(sh.n);
+		if (dot(nn, sh.d) > 0.0f) nn = nn * -1.0f;
+		const V3 dir = cosine_sample_hemisphere(si, sj);
+		float pdf = dir.z * (float)PSY_INV_PI_D;
+		const V3 out = zup_to_vec(dir, nn);
+		const Spec filter = lambert_eval(sh.col, sh.d, out, sh.n, wl);
+		WorldRayD wr;
+		wr.o = sh.p + sh.off;
+		wr.d = out;
+		wr.time = ps.time[slot];
+		wr.occl = false;
+		propagate_differentials(sh, &wr);
+		if (pdf < 0.00001f) pdf = 0.00001f;
+		for (int k = 0; k < 4; ++k) fcol.e[k] *= filter.e[k] / pdf;
+		store_ray(wb.ray[0], wb.cap, i, wr, 0.0f);
+		ps.dimstep[slot] = (dim & 0xffffu) | (step << 16);
+		ps.col[slot] = f4(col);
+		ps.fcol[slot] = f4(fcol);
+		ps.last_pdf[slot] = pdf;
+	}
 }
 
 // Adds each pixel's samples, in sample order, to the film; rejects
@@ -381,55 +491,78 @@ __global__ void film_reduce_kernel(RenderParams rp, PathSoA ps, float* xyz, uint
 	if (counts) counts[pixel] += c;
 }
 
-template <unsigned F>
-static int grid_for() {
-	int dev = 0, sms = 0, b0 = 0, b1 = 0, b2 = 0;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, step_kernel<STEP_CAMERA, F>, 128, 0);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, step_kernel<STEP_SHADOW, F>, 128, 0);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, step_kernel<STEP_BOUNCE, F>, 128, 0);
-	int b = b0;
-	if (b1 > 0 && b1 < b) b = b1;
-	if (b2 > 0 && b2 < b) b = b2;
-	if (b < 1) b = 1;
-	return sms * b;
+// ---------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------
+template <typename K>
+static int resident_blocks(K kernel) {
+	int b = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 128, 0);
+	return b < 1 ? 1 : b;
 }
 
-int render_grid(unsigned features) { return features == FEAT_FLAT ? grid_for<FEAT_FLAT>() : grid_for<FEAT_ALL>(); }
+struct WaveGrids {
+	int trace_c, trace_o, shade_c, shade_b, shadow;
+};
 
 template <unsigned F>
-static void launch_steps(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
-                         const WaveQueues& wq, unsigned* status, int grid, cudaStream_t st, uint32_t* launches) {
-	int* n_prev = nullptr;
-	const int* q_prev = nullptr;
-	for (int s = 0; s < (int)rp.path_length * 2; ++s) {
-		int* q_out = (s & 1) ? wq.q1 : wq.q0;
-		int* n_out = wq.counters + 2 * s;
-		int* work = wq.counters + 2 * s + 1;
-		if (s == 0)
-			step_kernel<STEP_CAMERA, F><<<grid, 128, 0, st>>>(sc, hd, rp, ps, nullptr, nullptr, q_out, n_out, work,
-			                                                   wq.rays, status);
-		else if (s & 1)
-			step_kernel<STEP_SHADOW, F><<<grid, 128, 0, st>>>(sc, hd, rp, ps, q_prev, n_prev, q_out, n_out, work,
-			                                                   wq.rays, status);
-		else
-			step_kernel<STEP_BOUNCE, F><<<grid, 128, 0, st>>>(sc, hd, rp, ps, q_prev, n_prev, q_out, n_out, work,
-			                                                   wq.rays, status);
-		++*launches;
-		q_prev = q_out;
-		n_prev = n_out;
+static WaveGrids grids_for() {
+	int dev = 0, sms = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	WaveGrids g;
+	g.trace_c = sms * resident_blocks(trace_wave_kernel<F, false>);
+	g.trace_o = sms * resident_blocks(trace_wave_kernel<F, true>);
+	g.shade_c = sms * resident_blocks(shade_hit_kernel<true, F>);
+	g.shade_b = sms * resident_blocks(shade_hit_kernel<false, F>);
+	g.shadow = sms * resident_blocks(shade_shadow_kernel);
+	return g;
+}
+
+// Counters per wave: [0] camera trace work, [1] camera shade work; per step
+// s >= 1 (shadow and bounce pairs) four more; see launch_wave.
+int render_counter_count(uint32_t path_length) { return 4 + 8 * (int)path_length; }
+
+template <unsigned F>
+static void launch_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
+                        const WaveBufs& wb, const WaveQueues& wq, unsigned* status, cudaStream_t st,
+                        uint32_t* launches) {
+	static const WaveGrids g = grids_for<F>();
+	const int P = rp.wave_paths;
+	int* c = wq.counters;
+	camera_gen_kernel<<<(P + 127) / 128, 128, 0, st>>>(sc, hd, rp, ps, wb);
+	trace_wave_kernel<F, false><<<g.trace_c, 128, 0, st>>>(sc, wb, wb.ray[0], nullptr, P, c + 0, wq.rays, status);
+	// camera hit -> shadow rays of the live paths into queue 0
+	int* q = wq.q0;
+	int* n = c + 2;
+	shade_hit_kernel<true, F><<<g.shade_c, 128, 0, st>>>(sc, hd, rp, ps, wb, nullptr, nullptr, P, q, n, c + 1, status);
+	*launches += 3;
+	c += 4;
+	for (uint32_t b = 0; b < rp.path_length; ++b) {
+		trace_wave_kernel<F, true><<<g.trace_o, 128, 0, st>>>(sc, wb, wb.ray[1], n, 0, c + 0, wq.rays, status);
+		shade_shadow_kernel<<<g.shadow, 128, 0, st>>>(hd, rp, ps, wb, q, n, c + 1);
+		*launches += 2;
+		if (b + 1 == rp.path_length) break;  // the last shadow step ends every path
+		trace_wave_kernel<F, false><<<g.trace_c, 128, 0, st>>>(sc, wb, wb.ray[0], n, 0, c + 2, wq.rays, status);
+		int* q2 = (q == wq.q0) ? wq.q1 : wq.q0;
+		int* n2 = c + 4;
+		shade_hit_kernel<false, F><<<g.shade_b, 128, 0, st>>>(sc, hd, rp, ps, wb, q, n, 0, q2, n2, c + 3, status);
+		*launches += 2;
+		q = q2;
+		n = n2;
+		c += 8;
 	}
 }
 
 cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
-                               const WaveQueues& wq, float* xyz, uint32_t* counts, unsigned* status, int grid,
-                               cudaStream_t st, uint32_t* launches) {
-	pix_init_kernel<<<(rp.wave_paths + 255) / 256, 256, 0, st>>>(rp, ps);
-	++*launches;
-	cudaMemsetAsync(wq.counters, 0, sizeof(int) * 2 * (rp.path_length * 2 + 1), st);
-	if (sc.features == FEAT_FLAT) launch_steps<FEAT_FLAT>(sc, hd, rp, ps, wq, status, grid, st, launches);
-	else launch_steps<FEAT_ALL>(sc, hd, rp, ps, wq, status, grid, st, launches);
+                               const WaveBufs& wb, const WaveQueues& wq, float* xyz, uint32_t* counts,
+                               unsigned* status, cudaStream_t st, uint32_t* launches) {
+	cudaMemsetAsync(wq.counters, 0, sizeof(int) * render_counter_count(rp.path_length), st);
+	switch (feature_variant(sc.features)) {
+		case FEAT_FLAT: launch_wave<FEAT_FLAT>(sc, hd, rp, ps, wb, wq, status, st, launches); break;
+		case FEAT_STILL: launch_wave<FEAT_STILL>(sc, hd, rp, ps, wb, wq, status, st, launches); break;
+		default: launch_wave<FEAT_ALL>(sc, hd, rp, ps, wb, wq, status, st, launches); break;
+	}
 	film_reduce_kernel<<<(rp.wave_paths / rp.spp + 127) / 128, 128, 0, st>>>(rp, ps, xyz, counts);
 	++*launches;
 	return cudaGetLastError();

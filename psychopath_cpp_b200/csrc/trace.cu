@@ -100,10 +100,11 @@ cudaError_t launch_trace(const DevScene& sc, const RaySoA& rays, const HitSoA& h
 	if (n == 0) return cudaSuccess;
 	const int block = 128;
 	const uint32_t grid = (n + block - 1) / block;
-	if (sc.features == FEAT_FLAT)
-		trace_kernel<FEAT_FLAT><<<grid, block, 0, stream>>>(sc, rays, hits, n, status);
-	else
-		trace_kernel<FEAT_ALL><<<grid, block, 0, stream>>>(sc, rays, hits, n, status);
+	switch (feature_variant(sc.features)) {
+		case FEAT_FLAT: trace_kernel<FEAT_FLAT><<<grid, block, 0, stream>>>(sc, rays, hits, n, status); break;
+		case FEAT_STILL: trace_kernel<FEAT_STILL><<<grid, block, 0, stream>>>(sc, rays, hits, n, status); break;
+		default: trace_kernel<FEAT_ALL><<<grid, block, 0, stream>>>(sc, rays, hits, n, status); break;
+	}
 	return cudaGetLastError();
 }
 

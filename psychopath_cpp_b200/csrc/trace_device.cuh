@@ -220,73 +220,6 @@ __device__ __forceinline__ float patch_vlen(const Patch<4>& q) { return longest_
 __device__ __forceinline__ float patch_ulen(const Patch<16>& q) { return longest_axis(q.p[0] - q.p[3]); }
 __device__ __forceinline__ float patch_vlen(const Patch<16>& q) { return longest_axis(q.p[0] - q.p[12]); }
 
-// Bilinear::split_u / split_v: p1 = first half (written in place), p2 = second half.
-__device__ __forceinline__ void patch_split_u(Patch<4>& p, Patch<4>* p2) {
-	const V3 m01 = (p.p[0] + p.p[1]) * 0.5f;
-	const V3 m23 = (p.p[2] + p.p[3]) * 0.5f;
-	p2->p[0] = m01;
-	p2->p[1] = p.p[1];
-	p2->p[2] = m23;
-	p2->p[3] = p.p[3];
-	p.p[1] = m01;
-	p.p[3] = m23;
-}
-__device__ __forceinline__ void patch_split_v(Patch<4>& p, Patch<4>* p2) {
-	const V3 m02 = (p.p[0] + p.p[2]) * 0.5f;
-	const V3 m13 = (p.p[1] + p.p[3]) * 0.5f;
-	p2->p[0] = m02;
-	p2->p[1] = m13;
-	p2->p[2] = p.p[2];
-	p2->p[3] = p.p[3];
-	p.p[2] = m02;
-	p.p[3] = m13;
-}
-
-// Bicubic::split_u / split_v (de Casteljau at 0.5 per row / column).
-__device__ __forceinline__ void patch_split_u(Patch<16>& p, Patch<16>* p2) {
-#pragma unroll
-	for (int r = 0; r < 4; ++r) {
-		const int rr = r * 4;
-		const V3 tmp = (p.p[rr + 1] + p.p[rr + 2]) * 0.5f;
-		const V3 q3 = p.p[rr + 3];
-		const V3 q2 = (p.p[rr + 3] + p.p[rr + 2]) * 0.5f;
-		const V3 q1 = (tmp + q2) * 0.5f;
-		const V3 a0 = p.p[rr + 0];
-		const V3 a1 = (p.p[rr + 0] + p.p[rr + 1]) * 0.5f;
-		const V3 a2 = (tmp + a1) * 0.5f;
-		const V3 a3 = (a2 + q1) * 0.5f;
-		p2->p[rr + 3] = q3;
-		p2->p[rr + 2] = q2;
-		p2->p[rr + 1] = q1;
-		p2->p[rr + 0] = a3;
-		p.p[rr + 0] = a0;
-		p.p[rr + 1] = a1;
-		p.p[rr + 2] = a2;
-		p.p[rr + 3] = a3;
-	}
-}
-__device__ __forceinline__ void patch_split_v(Patch<16>& p, Patch<16>* p2) {
-#pragma unroll
-	for (int c = 0; c < 4; ++c) {
-		const V3 tmp = (p.p[c + 4] + p.p[c + 8]) * 0.5f;
-		const V3 q3 = p.p[c + 12];
-		const V3 q2 = (p.p[c + 12] + p.p[c + 8]) * 0.5f;
-		const V3 q1 = (tmp + q2) * 0.5f;
-		const V3 a0 = p.p[c + 0];
-		const V3 a1 = (p.p[c + 0] + p.p[c + 4]) * 0.5f;
-		const V3 a2 = (tmp + a1) * 0.5f;
-		const V3 a3 = (a2 + q1) * 0.5f;
-		p2->p[c + 12] = q3;
-		p2->p[c + 8] = q2;
-		p2->p[c + 4] = q1;
-		p2->p[c + 0] = a3;
-		p.p[c + 0] = a0;
-		p.p[c + 4] = a1;
-		p.p[c + 8] = a2;
-		p.p[c + 12] = a3;
-	}
-}
-
 template <int NV>
 __device__ __forceinline__ void patch_load(const float* src, Patch<NV>* q) {
 #pragma unroll
@@ -298,9 +231,33 @@ struct PatchHit {
 	float t, u, v, max_dim;
 };
 
-// In-place halves of a split (Bilinear/Bicubic::split_u / split_v,
-// object/bilinear.hpp:59-82, object/bicubic.hpp:74-108): only the kept half
-// is written back, computed with the same operations as the full split.
+// Splits of a patch at the middle of u or v (Bilinear::split_u / split_v,
+// object/bilinear.hpp:59-82; Bicubic::split_u / split_v, de Casteljau at 0.5
+// per row or column, object/bicubic.hpp:74-108), with the reference's float
+// operations.  patch_split leaves the second half in `p` and writes the
+// first half to `f`; patch_half_u / patch_half_v keep one half in place and
+// give the same values for it.
+__device__ __forceinline__ void patch_split(Patch<4>& p, Patch<4>& f, bool along_u) {
+	if (along_u) {
+		const V3 m01 = (p.p[0] + p.p[1]) * 0.5f;
+		const V3 m23 = (p.p[2] + p.p[3]) * 0.5f;
+		f.p[0] = p.p[0];
+		f.p[1] = m01;
+		f.p[2] = p.p[2];
+		f.p[3] = m23;
+		p.p[0] = m01;
+		p.p[2] = m23;
+	} else {
+		const V3 m02 = (p.p[0] + p.p[2]) * 0.5f;
+		const V3 m13 = (p.p[1] + p.p[3]) * 0.5f;
+		f.p[0] = p.p[0];
+		f.p[1] = p.p[1];
+		f.p[2] = m02;
+		f.p[3] = m13;
+		p.p[0] = m02;
+		p.p[1] = m13;
+	}
+}
 __device__ __forceinline__ void patch_half_u(Patch<4>& p, bool second) {
 	const V3 m01 = (p.p[0] + p.p[1]) * 0.5f;
 	const V3 m23 = (p.p[2] + p.p[3]) * 0.5f;
@@ -323,8 +280,25 @@ __device__ __forceinline__ void patch_half_v(Patch<4>& p, bool second) {
 		p.p[3] = m13;
 	}
 }
-// One de Casteljau split at 0.5 of four control points a,b,c,d (a row or a
-// column of a bicubic patch), keeping one half.
+
+// One de Casteljau split at 0.5 of the control points a,b,c,d of a row or a
+// column: a..d become the second half, fa..fd the first.
+__device__ __forceinline__ void bezier_split(V3& a, V3& b, V3& c, V3& d, V3& fa, V3& fb, V3& fc, V3& fd) {
+	const V3 tmp = (b + c) * 0.5f;
+	const V3 q2 = (d + c) * 0.5f;
+	const V3 q1 = (tmp + q2) * 0.5f;
+	const V3 a1 = (a + b) * 0.5f;
+	const V3 a2 = (tmp + a1) * 0.5f;
+	const V3 a3 = (a2 + q1) * 0.5f;
+	fa = a;
+	fb = a1;
+	fc = a2;
+	fd = a3;
+	a = a3;
+	b = q1;
+	c = q2;
+}
+// The same split keeping one half in place.
 __device__ __forceinline__ void bezier_half(V3& a, V3& b, V3& c, V3& d, bool second) {
 	const V3 tmp = (b + c) * 0.5f;
 	const V3 q2 = (d + c) * 0.5f;
@@ -342,6 +316,18 @@ __device__ __forceinline__ void bezier_half(V3& a, V3& b, V3& c, V3& d, bool sec
 		d = a3;
 	}
 }
+__device__ __forceinline__ void patch_split(Patch<16>& p, Patch<16>& f, bool along_u) {
+	if (along_u) {
+#pragma unroll
+		for (int r = 0; r < 4; ++r)
+			bezier_split(p.p[r * 4], p.p[r * 4 + 1], p.p[r * 4 + 2], p.p[r * 4 + 3], f.p[r * 4], f.p[r * 4 + 1],
+			             f.p[r * 4 + 2], f.p[r * 4 + 3]);
+	} else {
+#pragma unroll
+		for (int c = 0; c < 4; ++c)
+			bezier_split(p.p[c], p.p[c + 4], p.p[c + 8], p.p[c + 12], f.p[c], f.p[c + 4], f.p[c + 8], f.p[c + 12]);
+	}
+}
 __device__ __forceinline__ void patch_half_u(Patch<16>& p, bool second) {
 #pragma unroll
 	for (int r = 0; r < 4; ++r) bezier_half(p.p[r * 4], p.p[r * 4 + 1], p.p[r * 4 + 2], p.p[r * 4 + 3], second);
@@ -351,7 +337,7 @@ __device__ __forceinline__ void patch_half_v(Patch<16>& p, bool second) {
 	for (int c = 0; c < 4; ++c) bezier_half(p.p[c], p.p[c + 4], p.p[c + 8], p.p[c + 12], second);
 }
 
-// Path of a node in the bisection tree: one bit per split.
+// Path of a node in the bisection tree: one bit per split level.
 struct Bits128 {
 	uint64_t lo, hi;
 	__device__ __forceinline__ bool get(int i) const { return i < 64 ? ((lo >> i) & 1ull) : ((hi >> (i - 64)) & 1ull); }
@@ -376,114 +362,174 @@ struct Bits128 {
 	__device__ __forceinline__ int popc() const { return __popcll(lo) + __popcll(hi); }
 };
 
+// Bounds of a sub-patch (each time sample) and the ray's test against them:
+// the top of the loop of intersect_rays_with_patch (object/patch_utils.hpp).
+template <int NV, int TSC>
+__device__ __forceinline__ bool patch_node_test(const Patch<NV> (&q)[TSC], float t_nalpha, const LocalRay& r,
+                                                float max_t, float* max_dim, float* h0, float* h1) {
+	Box bb[TSC];
+	float md = 0.0f;
+#pragma unroll
+	for (int k = 0; k < TSC; ++k) {
+		bb[k] = patch_bound<NV>(q[k]);
+		const float ld = longest_axis(bb[k].hi - bb[k].lo);
+		md = (k == 0) ? ld : smax(md, ld);
+	}
+	*max_dim = md;
+	if (TSC == 1) return box_hit(bb[0], r.o, r.dinv, max_t, h0, h1);
+	return box_hit(box_lerp(t_nalpha, bb[0], bb[TSC - 1]), r.o, r.dinv, max_t, h0, h1);
+}
+
+// Sub-patches stored on the current path: one every PSY_PATCH_CP_STEP
+// levels, for depths PSY_PATCH_CP_STEP .. PSY_PATCH_CP_STEP*PSY_PATCH_CP_COUNT.
+#define PSY_PATCH_CP_STEP 8
+#define PSY_PATCH_CP_COUNT 7
+
 // Per-ray bisection of one patch with TSC time samples (TSC = 1 or 2):
 // intersect_rays_with_patch for a single ray (object/patch_utils.hpp:18-200).
 //
-// The reference walks the split tree depth first, second half before first
-// half, keeping the pending first halves on a stack.  Here a node is its
-// path from the root (1 = second half) plus the split directions; when a
-// subtree is finished the deepest pending first half is rebuilt by replaying
-// the recorded splits from the root patch.  The replay performs the same
-// float operations as the first descent, so every node's control points and
-// uv range are bit-identical to the stored ones, and the walk needs no
-// per-ray stack of sub-patches.  The reference's stack index (its forced
-// leaf at 63) counts second halves only: the population count of the path.
+// The reference walks the split tree depth first with a stack of sub-patches:
+// a split pushes the first half, then the second, and the second half is
+// processed first.  Here both halves are tested against the ray when they
+// are made.  The second half is entered if its box is hit; the first half
+// is entered at once if only its box is hit, remembered as pending if both
+// are, and dropped if its box is missed (box_hit only gets stricter as the
+// ray's max t shrinks, so the reference would find it missed later as well).
+// A node is its path from the root (1 = second half) plus the split
+// directions; a pending first half is rebuilt when its turn comes by
+// replaying the recorded splits from the deepest stored ancestor on the path
+// (every PSY_PATCH_CP_STEP levels, else the root).  The replay performs the
+// same float operations as the first split, so every node's control points
+// and uv range are bit-identical to the reference's, the visiting order and
+// the leaf results are the same, and no per-ray stack of sub-patches is
+// needed.  The reference's stack index (its forced leaf at 63) is the number
+// of second halves on the path: the population count of the path bits.
 //
 // Returns true when a new closest hit was recorded (or, for occlusion rays,
 // when any leaf was hit).
 template <int NV, int TSC>
 __device__ bool patch_intersect(const float* verts, float time, const LocalRay& r, float* max_t, bool occl,
                                 float dice_rate, float min_upoly, PatchHit* hit) {
+	constexpr int CP = PSY_PATCH_CP_STEP;
+	constexpr int NCP = PSY_PATCH_CP_COUNT;
 	Patch<NV> cur[TSC];
 #pragma unroll
 	for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur[k]);
-	int t_index = 0;
 	float t_nalpha = 0.0f;
 	if (TSC > 1) {
+		// bounds are lerped between the two samples; time == 1.0 would index
+		// past the last sample in the reference (undefined) and gives the
+		// first sample's bounds here
 		const float t_time = time * (float)(TSC - 1);
-		t_index = (int)t_time;
-		t_nalpha = t_time - (float)t_index;
-		// time == 1.0 would index past the last sample (undefined in the
-		// reference); clamp to the last segment
-		if (t_index > TSC - 2) t_index = TSC - 2;
+		t_nalpha = t_time - (float)(int)t_time;
 	}
-	Bits128 path{0, 0}, dirs{0, 0};  // dirs bit: 1 = split along u
-	int depth = 0;                   // splits from the root
+	float max_dim, h0, h1;
+	if (!patch_node_test<NV, TSC>(cur, t_nalpha, r, *max_t, &max_dim, &h0, &h1)) return false;
+
+	Patch<NV> cps[NCP][TSC];
+	float cpuv[NCP][4];
+	Bits128 path{0, 0}, dirs{0, 0}, pend{0, 0};  // dirs bit: 1 = split along u
+	int depth = 0;                                // splits from the root
 	float u0 = 0.0f, u1 = 1.0f, v0 = 0.0f, v1 = 1.0f;
 	bool found = false;
 	while (true) {
-		Box bb[TSC];
-		float max_dim = 0.0f;
-#pragma unroll
-		for (int k = 0; k < TSC; ++k) {
-			bb[k] = patch_bound<NV>(cur[k]);
-			const float ld = longest_axis(bb[k].hi - bb[k].lo);
-			max_dim = (k == 0) ? ld : smax(max_dim, ld);
-		}
-		float h0, h1;
-		bool h;
-		if (TSC == 1) h = box_hit(bb[0], r.o, r.dinv, *max_t, &h0, &h1);
-		else h = box_hit(box_lerp(t_nalpha, bb[0], bb[TSC - 1]), r.o, r.dinv, *max_t, &h0, &h1);
-		bool descend = false;
-		if (h) {
-			const float width = smax(ray_min_width(r.w, h0, h1) * dice_rate, min_upoly);
-			if (max_dim <= width || path.popc() == PSY_SPLIT_STACK - 1 || depth == 127) {
-				const float tt = (h0 + h1) * 0.5f;
-				if (tt > 0.0f && tt < *max_t) {
-					found = true;
-					if (occl) return true;
-					*max_t = tt;
-					hit->t = tt;
-					hit->u = (u0 + u1) * 0.5f;
-					hit->v = (v0 + v1) * 0.5f;
-					hit->max_dim = max_dim;
-				}
-			} else {
-				descend = true;
+		// `cur` is a node whose box the ray hits; max_dim, h0, h1 are its test
+		const float width = smax(ray_min_width(r.w, h0, h1) * dice_rate, min_upoly);
+		bool entered = false;
+		if (max_dim <= width || path.popc() == PSY_SPLIT_STACK - 1 || depth == 127) {
+			const float tt = (h0 + h1) * 0.5f;
+			if (tt > 0.0f && tt < *max_t) {
+				found = true;
+				if (occl) return true;
+				*max_t = tt;
+				hit->t = tt;
+				hit->u = (u0 + u1) * 0.5f;
+				hit->v = (v0 + v1) * 0.5f;
+				hit->max_dim = max_dim;
 			}
-		}
-		if (descend) {
+		} else {
 			const bool along_u = patch_ulen(cur[0]) > patch_vlen(cur[0]);
-			if (along_u) {
+			Patch<NV> first[TSC];
 #pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_half_u(cur[k], true);
-				u0 = (u0 + u1) * 0.5f;
-			} else {
-#pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_half_v(cur[k], true);
-				v0 = (v0 + v1) * 0.5f;
-			}
-			path.set(depth, true);
+			for (int k = 0; k < TSC; ++k) patch_split(cur[k], first[k], along_u);
+			float smd, sh0, sh1, fmd, fh0, fh1;
+			const bool s_hit = patch_node_test<NV, TSC>(cur, t_nalpha, r, *max_t, &smd, &sh0, &sh1);
+			const bool f_hit = patch_node_test<NV, TSC>(first, t_nalpha, r, *max_t, &fmd, &fh0, &fh1);
 			dirs.set(depth, along_u);
-			++depth;
-			continue;
+			const float mid = along_u ? (u0 + u1) * 0.5f : (v0 + v1) * 0.5f;
+			if (s_hit) {
+				path.set(depth, true);
+				pend.set(depth, f_hit);
+				if (along_u) u0 = mid; else v0 = mid;
+				max_dim = smd;
+				h0 = sh0;
+				h1 = sh1;
+				entered = true;
+			} else if (f_hit) {
+				path.set(depth, false);
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) cur[k] = first[k];
+				if (along_u) u1 = mid; else v1 = mid;
+				max_dim = fmd;
+				h0 = fh0;
+				h1 = fh1;
+				entered = true;
+			}
+			if (entered) {
+				++depth;
+				if (depth % CP == 0 && depth / CP <= NCP) {
+					const int c = depth / CP - 1;
+#pragma unroll
+					for (int k = 0; k < TSC; ++k) cps[c][k] = cur[k];
+					cpuv[c][0] = u0; cpuv[c][1] = u1; cpuv[c][2] = v0; cpuv[c][3] = v1;
+				}
+				continue;
+			}
 		}
-		// the deepest pending first half
-		const int lvl = path.highest_below(depth);
-		if (lvl < 0) break;
-		path.set(lvl, false);
-		depth = lvl + 1;
-		path.truncate(depth);
-		dirs.truncate(depth);
+		// resume at the deepest pending first half whose box is still hit
+		while (true) {
+			const int j = pend.highest_below(depth);
+			if (j < 0) return found;
+			pend.set(j, false);
+			path.set(j, false);
+			depth = j + 1;
+			path.truncate(depth);
+			dirs.truncate(depth);
+			pend.truncate(depth);
+			int c = j / CP;
+			if (c > NCP) c = NCP;
+			if (c == 0) {
 #pragma unroll
-		for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur[k]);
-		u0 = 0.0f; u1 = 1.0f; v0 = 0.0f; v1 = 1.0f;
-		for (int j = 0; j < depth; ++j) {
-			const bool second_half = path.get(j);
-			if (dirs.get(j)) {
-#pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_half_u(cur[k], second_half);
-				const float um = (u0 + u1) * 0.5f;
-				if (second_half) u0 = um; else u1 = um;
+				for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur[k]);
+				u0 = 0.0f; u1 = 1.0f; v0 = 0.0f; v1 = 1.0f;
 			} else {
 #pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_half_v(cur[k], second_half);
-				const float vm = (v0 + v1) * 0.5f;
-				if (second_half) v0 = vm; else v1 = vm;
+				for (int k = 0; k < TSC; ++k) cur[k] = cps[c - 1][k];
+				u0 = cpuv[c - 1][0]; u1 = cpuv[c - 1][1]; v0 = cpuv[c - 1][2]; v1 = cpuv[c - 1][3];
 			}
+			for (int l = c * CP; l <= j; ++l) {
+				const bool second_half = path.get(l);  // 0 at level j: the first half
+				if (dirs.get(l)) {
+#pragma unroll
+					for (int k = 0; k < TSC; ++k) patch_half_u(cur[k], second_half);
+					const float um = (u0 + u1) * 0.5f;
+					if (second_half) u0 = um; else u1 = um;
+				} else {
+#pragma unroll
+					for (int k = 0; k < TSC; ++k) patch_half_v(cur[k], second_half);
+					const float vm = (v0 + v1) * 0.5f;
+					if (second_half) v0 = vm; else v1 = vm;
+				}
+			}
+			if (depth % CP == 0 && depth / CP <= NCP) {
+				const int s = depth / CP - 1;
+#pragma unroll
+				for (int k = 0; k < TSC; ++k) cps[s][k] = cur[k];
+				cpuv[s][0] = u0; cpuv[s][1] = u1; cpuv[s][2] = v0; cpuv[s][3] = v1;
+			}
+			if (patch_node_test<NV, TSC>(cur, t_nalpha, r, *max_t, &max_dim, &h0, &h1)) break;
 		}
 	}
-	return found;
 }
 
 // ---------------------------------------------------------------------
@@ -546,124 +592,158 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 		if (root != REF_EMPTY) node_stack[nsp++] = root;
 	}
 
-	bool done = false;
-	while (!done) {
-		// leave finished levels, restoring the ray of the enclosing level
-		while (NESTED && L > 0 && nsp == lv[L].stack_base) {
-			const bool changed = lvl_frame[L] != lvl_frame[L - 1];
-			--L;
-			if (changed) {
-				if (lvl_frame[L] >= 0) r = make_local_x(wr, frame_at_index_lerp(frames[lvl_frame[L]], wr.time));
-				else r = make_local(wr);
-			}
-		}
-		if (nsp == 0) break;
-		const int ref = node_stack[--nsp];
-		if (ref >= 0) {
-			// inner node: test the child boxes (BBox4::intersect_ray, basics/bbox.hpp:566-595)
-			const DevNode* nd = sc.nodes + ref;
-			float b[24];
-			const float4* q = reinterpret_cast<const float4*>(nd->b);
-#pragma unroll
-			for (int i = 0; i < 6; ++i) {
-				const float4 v = __ldg(q + i);
-				b[i * 4 + 0] = v.x; b[i * 4 + 1] = v.y; b[i * 4 + 2] = v.z; b[i * 4 + 3] = v.w;
-			}
-			const int4 ch = __ldg(reinterpret_cast<const int4*>(nd->child));
-			const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->nchild));
-			const int nch = meta.x;
-			const int ts = meta.y;
-			if (ts > 1) {
-				const SeqPos sp = seq_pos(wr.time, ts);
-				const float* e0 = sp.i0 == 0 ? nd->b : sc.node_extra + (size_t)(meta.z + sp.i0 - 1) * 24;
-				if (sp.single) {
-					for (int i = 0; i < 24; ++i) b[i] = e0[i];
-				} else {
-					const float* e1 = sc.node_extra + (size_t)(meta.z + sp.i0) * 24;
-					const float ia = one_minus(sp.nalpha);
-					for (int i = 0; i < 24; ++i) b[i] = (e0[i] * ia) + (e1[i] * sp.nalpha);
+	// The loop alternates two phases so that the lanes of a warp run each
+	// phase together: (A) traverse until the next object leaf, (B) test it.
+	// The closest hit does not depend on the order objects are tested in
+	// (a sub-patch's box lies inside its parent's, so max_t pruning only
+	// drops leaves that could not be closer), except for exact ties.
+	while (true) {
+		int gi = -1, local = 0, shader = -1;
+		uint64_t id = 0;
+		DevInstance inst;
+		bool abort = false;
+		while (true) {
+			gi = -1;
+			// leave finished levels, restoring the ray of the enclosing level
+			while (NESTED && L > 0 && nsp == lv[L].stack_base) {
+				const bool changed = lvl_frame[L] != lvl_frame[L - 1];
+				--L;
+				if (changed) {
+					if (lvl_frame[L] >= 0) r = make_local_x(wr, frame_at_index_lerp(frames[lvl_frame[L]], wr.time));
+					else r = make_local(wr);
 				}
 			}
-			const int ds0 = r.dinv.x < 0.0f, ds1 = r.dinv.y < 0.0f, ds2 = r.dinv.z < 0.0f;
-			float tnear[4];
-			int order[4];
-			int nhit = 0;
-			const int chv[4] = {ch.x, ch.y, ch.z, ch.w};
-#pragma unroll
-			for (int c = 0; c < 4; ++c) {
-				const float xlo = (b[(0 + ds0) * 4 + c] - r.o.x) * r.dinv.x;
-				const float xhi = (b[(1 - ds0) * 4 + c] - r.o.x) * r.dinv.x;
-				const float ylo = (b[(2 + ds1) * 4 + c] - r.o.y) * r.dinv.y;
-				const float yhi = (b[(3 - ds1) * 4 + c] - r.o.y) * r.dinv.y;
-				const float zlo = (b[(4 + ds2) * 4 + c] - r.o.z) * r.dinv.z;
-				const float zhi = (b[(5 - ds2) * 4 + c] - r.o.z) * r.dinv.z;
-				const float mins = vmax(vmax(xlo, ylo), vmax(zlo, 0.0f));
-				const float maxs = vmax(vmin(vmin(xhi, yhi), zhi), -INFINITY) * BBOX_MAXT_ADJUST;
-				if (c < nch && mins < max_t && mins <= maxs) {
-					// insertion by near distance (stable for ties)
-					int pos = nhit;
-					while (pos > 0 && tnear[pos - 1] > mins) {
-						tnear[pos] = tnear[pos - 1];
-						order[pos] = order[pos - 1];
-						--pos;
+			if (nsp == 0) break;
+			const int ref = node_stack[--nsp];
+			if (ref >= 0) {
+				// inner node: test the child boxes (BBox4::intersect_ray, basics/bbox.hpp:566-595)
+				const DevNode* nd = sc.nodes + ref;
+				float b[24];
+				const float4* q = reinterpret_cast<const float4*>(nd->b);
+	#pragma unroll
+				for (int i = 0; i < 6; ++i) {
+					const float4 v = __ldg(q + i);
+					b[i * 4 + 0] = v.x; b[i * 4 + 1] = v.y; b[i * 4 + 2] = v.z; b[i * 4 + 3] = v.w;
+				}
+				const int4 ch = __ldg(reinterpret_cast<const int4*>(nd->child));
+				const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->nchild));
+				const int nch = meta.x;
+				const int ts = meta.y;
+				if (ts > 1) {
+					const SeqPos sp = seq_pos(wr.time, ts);
+					const float* e0 = sp.i0 == 0 ? nd->b : sc.node_extra + (size_t)(meta.z + sp.i0 - 1) * 24;
+					if (sp.single) {
+	#pragma unroll
+						for (int i = 0; i < 24; ++i) b[i] = e0[i];
+					} else {
+						const float* e1 = sc.node_extra + (size_t)(meta.z + sp.i0) * 24;
+						const float ia = one_minus(sp.nalpha);
+	#pragma unroll
+						for (int i = 0; i < 24; ++i) b[i] = (e0[i] * ia) + (e1[i] * sp.nalpha);
 					}
-					tnear[pos] = mins;
-					order[pos] = chv[c];
-					++nhit;
 				}
-			}
-			if (nsp + nhit > PSY_NODE_STACK) {
-				err |= ERRF_STACK;
-				break;
-			}
-			for (int i = nhit - 1; i >= 0; --i) node_stack[nsp++] = order[i];
-			continue;
-		}
-
-		// leaf: one instance of the current level's assembly
-		const int local = leaf_instance(ref);
-		const int gi = lv[L].inst_base + local;
-		const DevInstance inst = sc.instances[gi];
-		const uint64_t id = id_push(lv[L].id, (uint64_t)local, lv[L].id_bits);
-		const int shader = inst.shader >= 0 ? inst.shader : lv[L].shader;
-		const Frame& parent = lvl_frame[L] >= 0 ? frames[lvl_frame[L]] : none;
-
-		if (NESTED && inst.kind == INST_ASSEMBLY) {
-			if (L + 1 >= PSY_MAX_LEVELS) {
-				err |= ERRF_LEVELS;
+				// slab tests of the four children; every array index below is a
+				// compile-time constant so the node stays in registers
+				const bool ds0 = r.dinv.x < 0.0f, ds1 = r.dinv.y < 0.0f, ds2 = r.dinv.z < 0.0f;
+				const int chv[4] = {ch.x, ch.y, ch.z, ch.w};
+				float tk[4];
+				int ck[4], sk[4];
+				int nhit = 0;
+	#pragma unroll
+				for (int c = 0; c < 4; ++c) {
+					const float x0 = b[0 * 4 + c], x1 = b[1 * 4 + c];
+					const float y0 = b[2 * 4 + c], y1 = b[3 * 4 + c];
+					const float z0 = b[4 * 4 + c], z1 = b[5 * 4 + c];
+					const float xlo = ((ds0 ? x1 : x0) - r.o.x) * r.dinv.x;
+					const float xhi = ((ds0 ? x0 : x1) - r.o.x) * r.dinv.x;
+					const float ylo = ((ds1 ? y1 : y0) - r.o.y) * r.dinv.y;
+					const float yhi = ((ds1 ? y0 : y1) - r.o.y) * r.dinv.y;
+					const float zlo = ((ds2 ? z1 : z0) - r.o.z) * r.dinv.z;
+					const float zhi = ((ds2 ? z0 : z1) - r.o.z) * r.dinv.z;
+					const float mins = vmax(vmax(xlo, ylo), vmax(zlo, 0.0f));
+					const float maxs = vmax(vmin(vmin(xhi, yhi), zhi), -INFINITY) * BBOX_MAXT_ADJUST;
+					const bool h = c < nch && mins < max_t && mins <= maxs;
+					// a hit has mins < max_t <= inf, so inf marks the misses
+					tk[c] = h ? mins : INFINITY;
+					ck[c] = chv[c];
+					sk[c] = c;
+					nhit += h ? 1 : 0;
+				}
+				// nearest first, ties in child order (a stable sort by distance)
+				auto cswap = [&](int a, int bb) {
+					if (tk[bb] < tk[a] || (tk[bb] == tk[a] && sk[bb] < sk[a])) {
+						const float t = tk[a]; tk[a] = tk[bb]; tk[bb] = t;
+						const int c = ck[a]; ck[a] = ck[bb]; ck[bb] = c;
+						const int q = sk[a]; sk[a] = sk[bb]; sk[bb] = q;
+					}
+				};
+				cswap(0, 1);
+				cswap(2, 3);
+				cswap(0, 2);
+				cswap(1, 3);
+				cswap(1, 2);
+				if (nsp + nhit > PSY_NODE_STACK) {
+					err |= ERRF_STACK;
+					abort = true;
+					break;
+				}
+				if (nhit > 3) node_stack[nsp++] = ck[3];
+				if (nhit > 2) node_stack[nsp++] = ck[2];
+				if (nhit > 1) node_stack[nsp++] = ck[1];
+				if (nhit > 0) node_stack[nsp++] = ck[0];
 				continue;
 			}
-			const DevAssembly as = sc.assemblies[inst.data];
-			if (as.root == REF_EMPTY) continue;
-			if (XFORM && inst.xform_count > 0) {
-				if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &frames[L + 1])) {
-					err |= ERRF_MOTION;
+
+			// leaf: one instance of the current level's assembly
+			local = leaf_instance(ref);
+			gi = lv[L].inst_base + local;
+			inst = sc.instances[gi];
+			id = id_push(lv[L].id, (uint64_t)local, lv[L].id_bits);
+			shader = inst.shader >= 0 ? inst.shader : lv[L].shader;
+
+			if (NESTED && inst.kind == INST_ASSEMBLY) {
+				const Frame& parent = lvl_frame[L] >= 0 ? frames[lvl_frame[L]] : none;
+				if (L + 1 >= PSY_MAX_LEVELS) {
+					err |= ERRF_LEVELS;
 					continue;
 				}
-				lvl_frame[L + 1] = L + 1;
-				r = make_local_x(wr, frame_at_index_lerp(frames[L + 1], wr.time));
-			} else {
-				lvl_frame[L + 1] = lvl_frame[L];
+				const DevAssembly as = sc.assemblies[inst.data];
+				if (as.root == REF_EMPTY) continue;
+				if (XFORM && inst.xform_count > 0) {
+					if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &frames[L + 1])) {
+						err |= ERRF_MOTION;
+						continue;
+					}
+					lvl_frame[L + 1] = L + 1;
+					r = make_local_x(wr, frame_at_index_lerp(frames[L + 1], wr.time));
+				} else {
+					lvl_frame[L + 1] = lvl_frame[L];
+				}
+				++L;
+				lv[L].asmb = inst.data;
+				lv[L].stack_base = nsp;
+				lv[L].shader = shader;
+				lv[L].inst = gi;
+				lv[L].id = id;
+				lv[L].id_bits = as.id_bits;
+				lv[L].inst_base = as.inst_base;
+				if (nsp + 1 > PSY_NODE_STACK) {
+					err |= ERRF_STACK;
+					abort = true;
+					break;
+				}
+				node_stack[nsp++] = as.root;
+				gi = -1;
+				continue;
 			}
-			++L;
-			lv[L].asmb = inst.data;
-			lv[L].stack_base = nsp;
-			lv[L].shader = shader;
-			lv[L].inst = gi;
-			lv[L].id = id;
-			lv[L].id_bits = as.id_bits;
-			lv[L].inst_base = as.inst_base;
-			if (nsp + 1 > PSY_NODE_STACK) {
-				err |= ERRF_STACK;
-				break;
-			}
-			node_stack[nsp++] = as.root;
-			continue;
+			break;  // an object instance
 		}
+		if (abort || gi < 0) break;
 
-		// object instance
+		// (B) the object instance's test
 		LocalRay lr = r;
 		if (XFORM && inst.xform_count > 0) {
+			const Frame& parent = lvl_frame[L] >= 0 ? frames[lvl_frame[L]] : none;
 			Frame nf;
 			if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &nf)) {
 				err |= ERRF_MOTION;
@@ -708,10 +788,7 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 			rec->kind = ob.kind;
 			rec->id = id;
 			rec->shader = shader;
-			if (wr.occl) {
-				done = true;
-				break;
-			}
+			if (wr.occl) break;
 			rec->t = ph.t;
 			rec->u = ph.u;
 			rec->v = ph.v;
