@@ -397,12 +397,169 @@ def run_trace_reference(args):
             "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+BATCH_METRIC = "paths/s batched (48 renders, one persistent wave stream + CUDA graph) vs plain (one render at a time)"
+
+
+def run_batch_ours(args, rank, local, pg, world):
+    """48 independent renders of uneven size: psy_render_batch (autotuned
+    wave length and block size, CUDA graph) against psy_render called once
+    per render, both timed with CUDA events over whole passes."""
+    import torch
+    from psychopath_cpp_b200 import api, scenes
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cfgs = scenes.batch_configs(48, seed=0)
+    ctxs, entries = [], []
+    for c in cfgs:
+        ctx = api.Context(local)
+        ctx.upload(scenes.batch_scene(c["seed"], c["res"], c["spp"], c["n_prims"], c["n_lights"]))
+        ctxs.append(ctx)
+        entries.append({"scene": ctx, "width": c["res"][0], "height": c["res"][1], "spp": c["spp"],
+                        "seed": c["seed"] + 1, "path_length": 4})
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    paths = sum(e["width"] * e["height"] * e["spp"] for e in entries)
+    # plain: one psy_render per render
+    integs = [api.PathTraceIntegrator(e["scene"], e["width"], e["height"], e["spp"], seed=e["seed"], path_length=4)
+              for e in entries]
+    films = [(torch.zeros(e["width"] * e["height"] * 3, dtype=torch.float32, device=dev),
+              torch.zeros(e["width"] * e["height"], dtype=torch.int32, device=dev)) for e in entries]
+
+    def plain_pass():
+        for it, (x, c) in zip(integs, films):
+            it.integrate_device(x, c, sp, with_stats=False)
+
+    def timed(fn, steps):
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(steps):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        return s.elapsed_time(e) / steps
+
+    for _ in range(args.warmup):
+        plain_pass()
+    plain_ms = timed(plain_pass, args.steps)
+    owner = api.Context(local)
+    b = api.BatchRenderer(owner, entries, use_graph=True)
+    tune = b.autotune(spp_divisor=16)
+    for _ in range(args.warmup):
+        b.render(sp, with_stats=False)
+    b.render(sp, with_stats=True)
+    launches = int(b.stats.launches)
+    rays = int(b.stats.rays)
+    with ClockSampler(local) as clk:
+        batch_ms = timed(lambda: b.render(sp, with_stats=False), args.steps)
+    owner.sync(sp)
+    value = paths / (batch_ms * 1e-3)
+    plain_value = paths / (plain_ms * 1e-3)
+    hbm, peak_kind = measured_peaks()
+    rbar = rays / paths
+    achieved = (rbar * BYTES_PER_CLOSEST_RAY + BYTES_PER_PATH_EXTRA) * paths / (batch_ms * 1e-3) / 1e9
+    return {
+        "metric": BATCH_METRIC, "value": round(value, 1), "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(batch_ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (48 seeded scenes: spheres + bilinear patches)",
+        "config": {"workload": "batch: 48 renders, 64x64..1024x768, 8-128 spp, 10-50,000 primitives, 1-100 lights, "
+                               "4 segments", "paths_per_step": paths, "tuned": tune,
+                   "l2": "per-wave path state larger than L2"},
+        "plain_paths_per_s": round(plain_value, 1), "plain_ms_per_step": round(plain_ms, 3),
+        "batched_over_plain": round(value / plain_value, 3), "mrays_per_s": round(rays / (batch_ms * 1e-3) / 1e6, 2),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 5), "traffic": None, "peak_source": peak_kind,
+                     "basis": "R*80 + 20 B per path (R = rays per path)"},
+        "gpu_launches": launches * args.steps, "clocks": clk.summary(),
+    }
+
+
+ADJOINT_METRIC = "adjoint/forward time ratio (path-replay adjoint vs differentiable forward render)"
+
+
+def run_adjoint_ours(args, rank, local, pg, world):
+    """Differentiable render at 256x256, 32 spp, 4 segments (the plain
+    scene's geometry with 8 lights; 256 albedo weights + 8 emission scales)
+    and its path-replay adjoint for an L2 image loss, timed with CUDA events."""
+    import numpy as np
+    import torch
+    from psychopath_cpp_b200 import api, scenes
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    res, spp = (256, 256), 32
+    sc = scenes.adjoint_scene(1, res=res, spp=spp)
+    ctx = api.Context(local)
+    ctx.upload(sc)
+    shaders, objects, ns, no = api.flat_indices(sc)
+    sp = np.full(ns, -1, np.int32)
+    op = np.full(no, -1, np.int32)
+    count = 0
+    init = []
+    for name in sorted((n for n in sc.root.shaders if n.startswith("mat")), key=lambda n: int(n[3:])):
+        sp[shaders[id(sc.root.shaders[name])]] = count
+        init += [0.8 * float(sc.root.shaders[name].color[0])] * 4
+        count += 4
+    for name in sorted((n for n in sc.root.objects if n.startswith("light")), key=lambda n: int(n[5:])):
+        op[objects[(0, name)]] = count
+        init.append(1.0)
+        count += 1
+    r = api.DiffRenderer(ctx, res[0], res[1], spp, sp, op, count, seed=1, path_length=4)
+    params = torch.tensor(init, dtype=torch.float32, device=dev)
+    rng = np.random.default_rng(0)
+    target_p = params + torch.from_numpy(rng.normal(0, 0.1, count).astype(np.float32)).to(dev)
+    tx, tc = r.forward(target_p)
+    target = tx.view(-1, 3) / tc.view(-1, 1).float()
+    stream = torch.cuda.current_stream(dev)
+    sp_ = stream.cuda_stream
+    xyz = torch.zeros(res[0] * res[1] * 3, dtype=torch.float32, device=dev)
+    cnt = torch.zeros(res[0] * res[1], dtype=torch.int32, device=dev)
+    grad = torch.zeros(count, dtype=torch.float32, device=dev)
+
+    def fwd():
+        xyz.zero_()
+        cnt.zero_()
+        r.forward(params, xyz, cnt, sp_)
+
+    def adj():
+        img = xyz.view(-1, 3) / cnt.view(-1, 1).float()
+        dl = (2.0 * (img - target) / cnt.view(-1, 1).float()).reshape(-1)
+        grad.zero_()
+        r.adjoint(params, dl, grad, sp_)
+
+    def timed(fn, steps):
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(steps):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        return s.elapsed_time(e) / steps
+
+    for _ in range(args.warmup):
+        fwd()
+        adj()
+    with ClockSampler(local) as clk:
+        f_ms = timed(fwd, args.steps)
+        a_ms = timed(adj, args.steps)
+    paths = res[0] * res[1] * spp
+    return {
+        "metric": ADJOINT_METRIC, "value": round(a_ms / f_ms, 4), "unit": "x", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(a_ms, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plain scene, 8 lights)",
+        "config": {"workload": "adjoint: 256x256, 32 spp, 4 segments, 256 albedo weights + 8 emission scales, "
+                               "L2 image loss", "paths_per_step": paths, "l2": "per-wave path state larger than L2"},
+        "forward_ms": round(f_ms, 3), "adjoint_ms": round(a_ms, 3),
+        "forward_paths_per_s": round(paths / (f_ms * 1e-3), 1), "clocks": clk.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="render", choices=["render", "trace"])
+    ap.add_argument("--workload", default="render", choices=["render", "trace", "batch", "adjoint"])
     ap.add_argument("--stream-paths", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -419,10 +576,14 @@ def main():
         return
     if args.workload == "render":
         res = run_render_ours(args, rank, local, pg, world)
+    elif args.workload == "batch":
+        res = run_batch_ours(args, rank, local, pg, world)
+    elif args.workload == "adjoint":
+        res = run_adjoint_ours(args, rank, local, pg, world)
     else:
         res = run_trace_ours(args, rank, local, pg, world)
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and args.workload in ("render", "trace"):
             res["cpu_baseline"] = render_cpu_baseline() if args.workload == "render" else trace_cpu_baseline()
         print(json.dumps(res))
     if pg:

@@ -310,6 +310,97 @@ typedef struct psy_render_stats {
 int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* counts, psy_render_stats* stats,
                void* stream);
 
+/* ------------------------------------------------------------------ */
+/* Differentiable rendering: parameters and the path-replay adjoint     */
+/* ------------------------------------------------------------------ */
+/*
+ * No counterpart in the reference, whose shading reads fixed RGB colours.
+ * A parameter vector (device memory) replaces chosen colours:
+ *  - a Lambert shader with shader_param[s] = p >= 0 takes its albedo
+ *    spectrum from four Gaussian basis weights params[p..p+3]:
+ *      a(lambda) = sum_k params[p+k] * exp(-(lambda - c_k)^2 / (2 s^2)),
+ *    c_k = PSY_ALBEDO_BASIS_C0 + k * PSY_ALBEDO_BASIS_STEP nm, s = PSY_ALBEDO_BASIS_SIGMA nm
+ *    (the RGB colour's upsampled spectrum is used where shader_param is -1);
+ *  - a sphere light with object_param[o] = q >= 0 has its emission scaled
+ *    by params[q].  Light selection keeps the uploaded energies, so the
+ *    estimator stays unbiased for any scale.
+ * With every entry -1 the render is the reference's.  Objects are numbered
+ * assembly by assembly in psy_scene_desc order, shaders as in the scene.
+ */
+#define PSY_ALBEDO_BASIS_C0 430.0f
+#define PSY_ALBEDO_BASIS_STEP 80.0f
+#define PSY_ALBEDO_BASIS_SIGMA 45.0f
+
+typedef struct psy_diff_desc {
+	uint32_t param_count;             /* length of params (and of the gradient) */
+	const float* params;              /* device, param_count floats */
+	uint32_t shader_count;            /* entries of shader_param: the scene's shader count */
+	const int32_t* shader_param;      /* host: first albedo weight of each shader, or -1 */
+	uint32_t object_count;            /* entries of object_param: the scene's object count */
+	const int32_t* object_param;      /* host: emission scale of each light object, or -1 */
+} psy_diff_desc;
+
+/* psy_render with the parameterised colours (same film semantics). */
+int psy_render_diff(psy_ctx* ctx, const psy_render_desc* desc, const psy_diff_desc* diff, float* xyz,
+                    uint32_t* counts, psy_render_stats* stats, void* stream);
+
+/*
+ * Path-replay adjoint of psy_render_diff: replays every path from its
+ * sampler seed (nothing is stored per vertex between the passes) and adds
+ * to grad (device, param_count floats) the gradient of a loss whose
+ * derivative with respect to the film sums is dl_dxyz (device,
+ * width*height*3 floats; the film sums are what psy_render_diff accumulates).
+ * The estimator is differentiated exactly: sampling decisions do not depend
+ * on the parameters.  Samples the film would reject (non-finite) are not
+ * excluded.  path_length must be at most PSY_ADJOINT_MAX_PATH.
+ */
+#define PSY_ADJOINT_MAX_PATH 8
+int psy_render_adjoint(psy_ctx* ctx, const psy_render_desc* desc, const psy_diff_desc* diff, const float* dl_dxyz,
+                       float* grad, psy_render_stats* stats, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Batched rendering                                                    */
+/* ------------------------------------------------------------------ */
+/*
+ * Many renders of different scenes in one stream of waves: the renders'
+ * paths are laid end to end and every wave takes the next paths of as many
+ * renders as fit, so small renders share the GPU instead of running one
+ * after another.  Each render's film gets exactly the samples psy_render
+ * would give it (same sampler sequence, same per-pixel order).
+ */
+typedef struct psy_batch_desc {
+	uint32_t count;                   /* renders */
+	psy_ctx* const* scenes;           /* per render: a context holding its uploaded scene, on ctx's device */
+	const psy_render_desc* renders;   /* per render: width, height, spp, seed, path_length */
+	float* const* xyz;                /* per render: device film, width*height*3 floats, accumulated */
+	uint32_t* const* counts;          /* per render: device sample counts, or NULL; the array may be NULL */
+	uint32_t stream_paths;            /* paths per wave; 0 = the context's tuned value, else 2^21 */
+	uint32_t block_size;              /* 64, 128 or 256 threads per block; 0 = tuned value, else 128 */
+	uint32_t use_graph;               /* 1: launch through a CUDA graph captured once and reused while
+	                                     the batch's launch parameters stay the same */
+} psy_batch_desc;
+
+/* Renders the batch on ctx's device (ctx owns the wave buffers and the
+ * graph; it may be one of the scene contexts).  Stream-ordered on `stream`;
+ * stats, when given, synchronises and reports the whole batch.  There is no
+ * single reference seam: it replaces running PathTraceIntegrator::integrate
+ * once per scene. */
+int psy_render_batch(psy_ctx* ctx, const psy_batch_desc* batch, psy_render_stats* stats, void* stream);
+
+typedef struct psy_batch_tuning {
+	uint32_t stream_paths;            /* chosen paths per wave */
+	uint32_t block_size;              /* chosen threads per block */
+	float ms;                         /* time of the chosen configuration on the tuning batch */
+	uint32_t trials;                  /* configurations timed */
+} psy_batch_tuning;
+
+/* Autotuner: times the batch with every sample count divided by
+ * spp_divisor (at least 1; scratch films, the batch's films are not
+ * touched) for waves of 2^14..2^20 paths and blocks of 64, 128 and 256
+ * threads, keeps the fastest in ctx for psy_render_batch calls whose
+ * configuration fields are 0, and returns it.  Synchronous. */
+int psy_batch_autotune(psy_ctx* ctx, const psy_batch_desc* batch, uint32_t spp_divisor, psy_batch_tuning* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,6 +93,22 @@ class RenderDesc(C.Structure):
                 ("path_length", C.c_uint32), ("stream_paths", C.c_uint32), ("block_size", C.c_uint32)]
 
 
+class DiffDesc(C.Structure):
+    _fields_ = [("param_count", C.c_uint32), ("params", C.POINTER(C.c_float)), ("shader_count", C.c_uint32),
+                ("shader_param", C.POINTER(C.c_int32)), ("object_count", C.c_uint32),
+                ("object_param", C.POINTER(C.c_int32))]
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("scenes", C.POINTER(C.c_void_p)), ("renders", C.POINTER(RenderDesc)),
+                ("xyz", C.POINTER(C.c_void_p)), ("counts", C.POINTER(C.c_void_p)), ("stream_paths", C.c_uint32),
+                ("block_size", C.c_uint32), ("use_graph", C.c_uint32)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("stream_paths", C.c_uint32), ("block_size", C.c_uint32), ("ms", C.c_float), ("trials", C.c_uint32)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("launches", C.c_uint32), ("waves", C.c_uint32)]
 
@@ -100,7 +116,8 @@ class RenderStats(C.Structure):
 # every symbol declared in include/psy_b200.h
 EXPORTED = ["psy_ctx_create", "psy_ctx_destroy", "psy_last_error", "psy_version", "psy_scene_upload",
             "psy_scene_stats_get", "psy_build_bvh4", "psy_build_light_tree", "psy_trace", "psy_trace_host", "psy_sync",
-            "psy_trace_host_noalloc",
+            "psy_trace_host_noalloc", "psy_render_batch", "psy_batch_autotune", "psy_render_diff",
+            "psy_render_adjoint",
             "psy_light_sample", "psy_render"]
 
 _lib = None
@@ -126,6 +143,14 @@ def load():
     L.psy_trace.argtypes = [C.c_void_p, C.POINTER(RaySoA), C.c_uint32, C.POINTER(HitSoA), C.c_void_p]
     L.psy_trace_host.argtypes = [C.c_void_p, C.POINTER(RaySoA), C.c_uint32, C.POINTER(HitSoA)]
     L.psy_sync.argtypes = [C.c_void_p, C.c_void_p]
+    if hasattr(L, "psy_render_diff"):
+        L.psy_render_diff.argtypes = [C.c_void_p, C.POINTER(RenderDesc), C.POINTER(DiffDesc), C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+        L.psy_render_adjoint.argtypes = [C.c_void_p, C.POINTER(RenderDesc), C.POINTER(DiffDesc), C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]
+    if hasattr(L, "psy_render_batch"):
+        L.psy_render_batch.argtypes = [C.c_void_p, C.POINTER(BatchDesc), C.c_void_p, C.c_void_p]
+        L.psy_batch_autotune.argtypes = [C.c_void_p, C.POINTER(BatchDesc), C.c_uint32, C.POINTER(BatchTuning)]
     if hasattr(L, "psy_trace_host_noalloc"):
         L.psy_trace_host_noalloc.argtypes = [C.c_void_p, C.POINTER(RaySoA), C.c_uint32, C.POINTER(HitSoA),
                                              C.c_void_p]

@@ -374,3 +374,133 @@ class PathTraceIntegrator:
         self.integrate_device(xyz, cnt)
         self.ctx.sync()
         return xyz.cpu().numpy().reshape(h, w, 3), cnt.cpu().numpy().reshape(h, w).astype(np.uint32)
+
+
+class BatchRenderer:
+    """Many renders of different scenes in one stream of waves
+    (psy_render_batch).  `entries` are dicts with `scene` (a Context holding
+    the uploaded scene), `width`, `height`, `spp`, `seed` and `path_length`.
+    Films are device tensors owned by this object, accumulated by each
+    render() call."""
+
+    def __init__(self, ctx: Context, entries: List[dict], stream_paths: int = 0, block_size: int = 0,
+                 use_graph: bool = True):
+        torch = _torch()
+        dev = torch.device("cuda", ctx.device)
+        self.ctx = ctx
+        self.entries = entries
+        n = len(entries)
+        self.films = [torch.zeros(e["height"] * e["width"] * 3, dtype=torch.float32, device=dev) for e in entries]
+        self.counts = [torch.zeros(e["height"] * e["width"], dtype=torch.int32, device=dev) for e in entries]
+        self._scenes = (C.c_void_p * n)(*[e["scene"].h.value for e in entries])
+        self._renders = (_abi.RenderDesc * n)(*[
+            _abi.RenderDesc(e["width"], e["height"], e["spp"], e.get("seed", 1), e.get("path_length", 4), 0, 0)
+            for e in entries])
+        self._xyz = (C.c_void_p * n)(*[f.data_ptr() for f in self.films])
+        self._cnt = (C.c_void_p * n)(*[c.data_ptr() for c in self.counts])
+        self.desc = _abi.BatchDesc(n, C.cast(self._scenes, C.POINTER(C.c_void_p)),
+                                   C.cast(self._renders, C.POINTER(_abi.RenderDesc)),
+                                   C.cast(self._xyz, C.POINTER(C.c_void_p)), C.cast(self._cnt, C.POINTER(C.c_void_p)),
+                                   stream_paths, block_size, 1 if use_graph else 0)
+        self.stats = _abi.RenderStats()
+
+    @property
+    def paths(self) -> int:
+        return sum(e["width"] * e["height"] * e["spp"] for e in self.entries)
+
+    def zero(self) -> None:
+        for f in self.films:
+            f.zero_()
+        for c in self.counts:
+            c.zero_()
+
+    def render(self, stream=None, with_stats: bool = True) -> None:
+        self.ctx.check(self.ctx.L.psy_render_batch(self.ctx.h, C.byref(self.desc),
+                                                   C.byref(self.stats) if with_stats else None, stream))
+
+    def autotune(self, spp_divisor: int = 16) -> dict:
+        t = _abi.BatchTuning()
+        self.ctx.check(self.ctx.L.psy_batch_autotune(self.ctx.h, C.byref(self.desc), spp_divisor, C.byref(t)))
+        return {"stream_paths": t.stream_paths, "block_size": t.block_size, "ms": t.ms, "trials": t.trials}
+
+    def images(self) -> List[Tuple[np.ndarray, np.ndarray]]:
+        _torch().cuda.synchronize(self.ctx.device)
+        out = []
+        for e, f, c in zip(self.entries, self.films, self.counts):
+            out.append((f.cpu().numpy().reshape(e["height"], e["width"], 3),
+                        c.cpu().numpy().reshape(e["height"], e["width"]).astype(np.uint32)))
+        return out
+
+
+def flat_indices(scene: Scene) -> Tuple[Dict[int, int], Dict[Tuple[int, str], int], int, int]:
+    """The scene indices flatten() gives shaders and objects: shader index by
+    id(SurfaceShader), object index by (assembly position, object name), and
+    the two counts.  Assemblies are numbered depth first from the root."""
+    asm_order: List[Assembly] = []
+
+    def collect(a: Assembly):
+        asm_order.append(a)
+        for sub in a.assemblies.values():
+            collect(sub)
+
+    collect(scene.root)
+    shaders: Dict[int, int] = {}
+    objects: Dict[Tuple[int, str], int] = {}
+    for ai, a in enumerate(asm_order):
+        for name in a.objects:
+            objects[(ai, name)] = len(objects)
+        for inst in a.instances:
+            sh = a.find_shader(inst.shader) if inst.shader is not None else None
+            if sh is not None and id(sh) not in shaders:
+                shaders[id(sh)] = len(shaders)
+    return shaders, objects, len(shaders), len(objects)
+
+
+class DiffRenderer:
+    """Differentiable render of the context's scene (psy_render_diff) and its
+    path-replay adjoint (psy_render_adjoint).  shader_param / object_param
+    map scene shaders and objects (flat_indices order) to parameter indices
+    (-1 = fixed): a shader gets 4 albedo basis weights, a light one emission
+    scale."""
+
+    def __init__(self, ctx: Context, width: int, height: int, spp: int, shader_param, object_param,
+                 param_count: int, seed: int = 1, path_length: int = 4, stream_paths: int = 0):
+        self.ctx = ctx
+        self.desc = _abi.RenderDesc(width, height, spp, seed, path_length, stream_paths, 0)
+        self.param_count = int(param_count)
+        self._sp = np.ascontiguousarray(np.asarray(shader_param, np.int32))
+        self._op = np.ascontiguousarray(np.asarray(object_param, np.int32))
+        self.stats = _abi.RenderStats()
+
+    def _diff(self, params) -> _abi.DiffDesc:
+        assert params.dtype == _torch().float32 and params.is_cuda and params.numel() == self.param_count
+        return _abi.DiffDesc(self.param_count, C.cast(C.c_void_p(params.data_ptr()), _abi.fp),
+                             len(self._sp), self._sp.ctypes.data_as(C.POINTER(C.c_int32)),
+                             len(self._op), self._op.ctypes.data_as(C.POINTER(C.c_int32)))
+
+    def forward(self, params, xyz=None, counts=None, stream=None, with_stats: bool = False):
+        """Film sums (h*w*3) and counts (h*w) of one render, as device tensors."""
+        torch = _torch()
+        dev = torch.device("cuda", self.ctx.device)
+        n = self.desc.width * self.desc.height
+        if xyz is None:
+            xyz = torch.zeros(n * 3, dtype=torch.float32, device=dev)
+        if counts is None:
+            counts = torch.zeros(n, dtype=torch.int32, device=dev)
+        d = self._diff(params)
+        self.ctx.check(self.ctx.L.psy_render_diff(self.ctx.h, C.byref(self.desc), C.byref(d),
+                                                  C.c_void_p(xyz.data_ptr()), C.c_void_p(counts.data_ptr()),
+                                                  C.byref(self.stats) if with_stats else None, stream))
+        return xyz, counts
+
+    def adjoint(self, params, dl_dxyz, grad=None, stream=None, with_stats: bool = False):
+        """Adds dL/dparams to grad (a new zero tensor when None) and returns it."""
+        torch = _torch()
+        if grad is None:
+            grad = torch.zeros(self.param_count, dtype=torch.float32, device=params.device)
+        dl = dl_dxyz.contiguous().to(torch.float32)
+        d = self._diff(params)
+        self.ctx.check(self.ctx.L.psy_render_adjoint(self.ctx.h, C.byref(self.desc), C.byref(d),
+                                                     C.c_void_p(dl.data_ptr()), C.c_void_p(grad.data_ptr()),
+                                                     C.byref(self.stats) if with_stats else None, stream))
+        return grad

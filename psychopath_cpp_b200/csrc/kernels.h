@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/psy_b200.h"
 #include "psy_scene.h"
 
 namespace psy {
@@ -35,13 +36,35 @@ struct HaltonDev {
 	const double* cmul;
 };
 
+// Parameters of one render (PathTraceIntegrator's settings and its film).
 struct RenderParams {
 	uint32_t width, height, spp, seed, path_length;
 	uint32_t light_count;    // root LightTree::light_count()
-	uint64_t wave_base;      // first global path (sample) index of the wave
-	int wave_paths;          // paths in this wave (a multiple of spp)
 	float min_x, max_x, min_y, max_y;  // film extent (renderer/renderer.cpp:52-55)
 	float ident_inv;         // diagonal of the reference's inverse of the identity
+	uint64_t path_base;      // first global path index of the render (0 unless batched)
+	uint64_t pixel_base;     // first global pixel index of the render (0 unless batched)
+	float* xyz;              // film XYZ sums, width * height * 3
+	uint32_t* counts;        // film sample counts (may be null)
+	// differentiable rendering (all null in plain renders)
+	const float* params;     // parameter vector
+	const int* shader_param; // per scene shader: first of its 4 albedo weights, or -1
+	const int* object_param; // per scene object: its emission scale, or -1
+	const float* dl_dxyz;    // adjoint: dL / d(film sums), width * height * 3
+	float* grad;             // adjoint: gradient accumulator, param_count floats
+	int param_count;
+	int grad_in_smem;        // adjoint: accumulate per block in shared memory first
+};
+
+// Largest path_length of the adjoint (vertex records per path).
+#define PSY_ADJ_MAX_VERTS 8
+
+// The global paths one wave covers: whole pixels, in order.
+struct WaveRange {
+	uint64_t base;           // first global path index
+	uint64_t pix_base;       // first global pixel index
+	int paths;
+	int pixels;
 };
 
 // Path state of one wave, structure of arrays (PTState,
@@ -58,6 +81,12 @@ struct PathSoA {
 	float* hit;         // stored intersection, 16 floats per path
 	float* pray;        // previous ray, 16 floats per path
 	float* sample;      // film sample XYZ, 3 floats per path
+	uint16_t* rid;      // render of the path (batches)
+	// adjoint pass only
+	float4* adj;        // dL / d(sample spectrum) per hero wavelength
+	float4* valb;       // albedo spectrum of each parameterised vertex, PSY_ADJ_MAX_VERTS per path
+	int* vpid;          // its first albedo weight (-1: not parameterised), PSY_ADJ_MAX_VERTS per path
+	int* nee_param;     // emission scale of the light sampled at the current vertex, or -1
 };
 
 // Rays and hits of a wave by queue position (cap = the wave's path capacity).
@@ -85,9 +114,20 @@ struct LightSampleSoADev {
 };
 
 int render_counter_count(uint32_t path_length);
-cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
-                               const WaveBufs& wb, const WaveQueues& wq, float* xyz, uint32_t* counts,
-                               unsigned* status, cudaStream_t st, uint32_t* launches);
+
+// One wave of a single render: scene and parameters go in kernel parameters.
+cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const WaveRange& wr,
+                               const PathSoA& ps, const WaveBufs& wb, const WaveQueues& wq, unsigned* status,
+                               int block, cudaStream_t st, uint32_t* launches);
+
+// One wave of a batch: the render of each path is found in device arrays
+// (scenes and renders, count entries each); features is the union of the
+// scenes' FEAT_* bits and max_path_length the largest path_length.
+cudaError_t launch_batch_wave(const DevScene* scenes, const RenderParams* renders, int count, unsigned features,
+                              uint32_t max_path_length, const HaltonDev& hd, const WaveRange& wr, const PathSoA& ps,
+                              const WaveBufs& wb, const WaveQueues& wq, unsigned* status, int block,
+                              cudaStream_t st, uint32_t* launches);
+
 cudaError_t launch_light_sample(const DevScene& sc, const LightQuerySoADev& q, const LightSampleSoADev& o, uint32_t n,
                                 float ident_inv, unsigned* status, cudaStream_t st);
 

@@ -43,6 +43,8 @@ psy_ctx::~psy_ctx() {
 	for (void* p : const_allocs) cudaFree(p);
 	if (d_status) cudaFree(d_status);
 	if (h_status) cudaFreeHost(h_status);
+	if (batch_graph) cudaGraphExecDestroy(batch_graph);
+	if (capture_stream) cudaStreamDestroy(capture_stream);
 }
 
 void psy_ctx::free_scene() {
@@ -100,7 +102,346 @@ int psy_ctx::check_status(cudaStream_t stream) {
 	return PSY_OK;
 }
 
+// ---------------------------------------------------------------------
+// Rendering helpers
+// ---------------------------------------------------------------------
+static int check_render(psy_ctx* ctx, const psy_render_desc* desc, const char* who) {
+	if (!ctx->has_scene) return ctx_fail(ctx, PSY_ERR_NO_SCENE, "%s: no scene uploaded", who);
+	if (desc->width == 0 || desc->height == 0 || desc->width > 65535 || desc->height > 65535)
+		return ctx_fail(ctx, PSY_ERR_ARG, "%s: resolution must be 1..65535 per axis", who);
+	if (desc->spp == 0 || desc->spp > 65535) return ctx_fail(ctx, PSY_ERR_ARG, "%s: spp must be 1..65535", who);
+	if (desc->path_length > 40) return ctx_fail(ctx, PSY_ERR_ARG, "%s: path_length must be at most 40", who);
+	if (ctx->host->assemblies[0].light_root < 0)
+		return ctx_fail(ctx, PSY_ERR_ARG, "%s: the scene has no lights (the reference integrator needs one)", who);
+	return PSY_OK;
+}
+
+static RenderParams render_params(const psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* counts) {
+	RenderParams rp;
+	rp.width = desc->width;
+	rp.height = desc->height;
+	rp.spp = desc->spp;
+	rp.seed = desc->seed;
+	rp.path_length = desc->path_length ? desc->path_length : 4;
+	rp.light_count = (uint32_t)ctx->host->assemblies[0].light_count;
+	rp.min_x = -1.0f;
+	rp.max_x = 1.0f;
+	rp.max_y = (float)desc->height / (float)desc->width;
+	rp.min_y = -rp.max_y;
+	rp.ident_inv = ctx->ident_inv;
+	rp.path_base = 0;
+	rp.pixel_base = 0;
+	rp.xyz = xyz;
+	rp.counts = counts;
+	rp.params = nullptr;
+	rp.shader_param = nullptr;
+	rp.object_param = nullptr;
+	rp.dl_dxyz = nullptr;
+	rp.grad = nullptr;
+	rp.param_count = 0;
+	rp.grad_in_smem = 0;
+	return rp;
+}
+
+// Path state, ray / hit buffers and queues for waves of P paths, in the
+// context's scratch buffers named with `prefix`.
+struct WaveSet {
+	PathSoA ps;
+	WaveBufs wb;
+	WaveQueues wq;
+};
+
+static int wave_set(psy_ctx* ctx, const char* prefix, uint64_t P, uint32_t path_length, WaveSet* ws,
+                    bool adjoint = false) {
+	int rc = PSY_OK;
+	std::string pre(prefix);
+	auto buf = [&](const char* name, size_t bytes) -> void* {
+		return ctx->scratch_buffer((pre + name).c_str(), bytes, &rc);
+	};
+	PathSoA& ps = ws->ps;
+	ps.smp = (uint32_t*)buf("smp", P * 4);
+	ps.dimstep = (uint32_t*)buf("dimstep", P * 4);
+	ps.wl = (float*)buf("wl", P * 4);
+	ps.time = (float*)buf("time", P * 4);
+	ps.last_pdf = (float*)buf("lpdf", P * 4);
+	ps.col = (float4*)buf("col", P * 16);
+	ps.fcol = (float4*)buf("fcol", P * 16);
+	ps.lcol = (float4*)buf("lcol", P * 16);
+	ps.hit = (float*)buf("hit", P * 64);
+	ps.pray = (float*)buf("pray", P * 64);
+	ps.sample = (float*)buf("sample", P * 12);
+	ps.rid = (uint16_t*)buf("rid", P * 2);
+	ps.adj = nullptr;
+	ps.valb = nullptr;
+	ps.vpid = nullptr;
+	ps.nee_param = nullptr;
+	if (adjoint) {
+		ps.adj = (float4*)buf("adj", P * 16);
+		ps.valb = (float4*)buf("valb", P * 16 * PSY_ADJ_MAX_VERTS);
+		ps.vpid = (int*)buf("vpid", P * 4 * PSY_ADJ_MAX_VERTS);
+		ps.nee_param = (int*)buf("neep", P * 4);
+		if (!ps.adj || !ps.valb || !ps.vpid || !ps.nee_param) return rc ? rc : PSY_ERR_OOM;
+	}
+	WaveQueues& wq = ws->wq;
+	wq.q0 = (int*)buf("q0", P * 4);
+	wq.q1 = (int*)buf("q1", P * 4);
+	wq.counters = (int*)buf("counters", sizeof(int) * render_counter_count(path_length));
+	wq.rays = (unsigned long long*)buf("rays", sizeof(unsigned long long));
+	WaveBufs& wb = ws->wb;
+	wb.cap = (int)P;
+	wb.ray[0] = (float4*)buf("ray0", P * 80);
+	wb.ray[1] = (float4*)buf("ray1", P * 80);
+	wb.hit_f = (float4*)buf("hitf", P * 16);
+	wb.hit_i = (int4*)buf("hiti", P * 48);
+	wb.occl = (uint8_t*)buf("occl", P);
+	if (!ps.smp || !ps.dimstep || !ps.wl || !ps.time || !ps.last_pdf || !ps.col || !ps.fcol || !ps.lcol ||
+	    !ps.hit || !ps.pray || !ps.sample || !ps.rid || !wq.q0 || !wq.q1 || !wq.counters || !wq.rays || !wb.ray[0] ||
+	    !wb.ray[1] || !wb.hit_f || !wb.hit_i || !wb.occl)
+		return rc ? rc : PSY_ERR_OOM;
+	return PSY_OK;
+}
+
+// One render in waves of P paths (a multiple of spp), on the context's
+// "r_" scratch buffers.
+static int render_single(psy_ctx* ctx, const psy_render_desc* desc, const RenderParams& rp, bool adjoint,
+                         psy_render_stats* stats, cudaStream_t st) {
+	cudaSetDevice(ctx->device);
+	int rc;
+	const uint64_t total = (uint64_t)desc->width * desc->height * desc->spp;
+	uint64_t want = desc->stream_paths ? desc->stream_paths : (1ull << 21);
+	if (want > (1ull << 26)) want = 1ull << 26;
+	uint64_t P = (want / desc->spp) * desc->spp;
+	if (P < desc->spp) P = desc->spp;
+	if (P > total) P = total;
+	WaveSet ws;
+	if ((rc = wave_set(ctx, "r_", P, rp.path_length, &ws, adjoint))) return rc;
+	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, sizeof(unsigned long long), st), "memset"))) return rc;
+	uint32_t launches = 0, waves = 0;
+	for (uint64_t base = 0; base < total; base += P) {
+		WaveRange wv;
+		wv.base = base;
+		wv.paths = (int)((total - base) < P ? (total - base) : P);
+		wv.pix_base = base / desc->spp;
+		wv.pixels = wv.paths / (int)desc->spp;
+		if ((rc = ctx_cuda(ctx,
+		                   launch_render_wave(ctx->dev, ctx->halton, rp, wv, ws.ps, ws.wb, ws.wq, ctx->d_status,
+		                                      (int)desc->block_size, st, &launches),
+		                   "render launch")))
+			return rc;
+		++waves;
+	}
+	if (stats) {
+		unsigned long long rays = 0;
+		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(&rays, ws.wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
+			return rc;
+		if ((rc = ctx->check_status(st))) return rc;
+		stats->paths = total;
+		stats->rays = rays;
+		stats->launches = launches;
+		stats->waves = waves;
+	}
+	return PSY_OK;
+}
+
+// Validates a parameter description against the scene and uploads its
+// index tables into rp.
+static int diff_params(psy_ctx* ctx, const psy_diff_desc* d, const char* who, RenderParams* rp) {
+	const size_t ns = ctx->host->shaders.size(), no = ctx->host->objects.size();
+	if (!d->params && d->param_count) return ctx_fail(ctx, PSY_ERR_ARG, "%s: params is NULL", who);
+	if (d->shader_count != ns || (ns && !d->shader_param))
+		return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader_param must have one entry per scene shader (%zu)", who, ns);
+	if (d->object_count != no || (no && !d->object_param))
+		return ctx_fail(ctx, PSY_ERR_ARG, "%s: object_param must have one entry per scene object (%zu)", who, no);
+	const int pc = (int)d->param_count;
+	for (size_t i = 0; i < ns; ++i) {
+		const int p = d->shader_param[i];
+		if (p < -1 || (p >= 0 && p + 3 >= pc))
+			return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader %zu's albedo weights %d..%d are outside the %d parameters", who,
+			                i, p, p + 3, pc);
+		if (p >= 0 && ctx->host->shaders[i].kind != SHADER_LAMBERT)
+			return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader %zu is not Lambert", who, i);
+	}
+	for (size_t i = 0; i < no; ++i) {
+		const int p = d->object_param[i];
+		if (p < -1 || p >= pc) return ctx_fail(ctx, PSY_ERR_ARG, "%s: object %zu's parameter %d is out of range", who, i, p);
+		if (p >= 0 && ctx->host->objects[i].kind != OBJ_SPHERE_LIGHT)
+			return ctx_fail(ctx, PSY_ERR_ARG, "%s: object %zu is not a light", who, i);
+	}
+	int rc;
+	int* sp = static_cast<int*>(ctx->scratch_buffer("d_spar", sizeof(int) * (ns ? ns : 1), &rc));
+	if (!sp) return rc;
+	int* op = static_cast<int*>(ctx->scratch_buffer("d_opar", sizeof(int) * (no ? no : 1), &rc));
+	if (!op) return rc;
+	if (ns && (rc = ctx_cuda(ctx, cudaMemcpy(sp, d->shader_param, sizeof(int) * ns, cudaMemcpyHostToDevice), who)))
+		return rc;
+	if (no && (rc = ctx_cuda(ctx, cudaMemcpy(op, d->object_param, sizeof(int) * no, cudaMemcpyHostToDevice), who)))
+		return rc;
+	rp->params = d->params;
+	rp->shader_param = sp;
+	rp->object_param = op;
+	rp->param_count = pc;
+	return PSY_OK;
+}
+
+// The batch: renders laid end to end in one global path space, rendered in
+// waves of at most P paths that end on pixel boundaries.
+static int render_batch(psy_ctx* ctx, const psy_batch_desc* b, psy_render_stats* stats, cudaStream_t st) {
+	if (b->count == 0) return PSY_OK;
+	if (!b->scenes || !b->renders || !b->xyz)
+		return ctx_fail(ctx, PSY_ERR_ARG, "psy_render_batch: scenes, renders and xyz are required");
+	if (b->count > 65535) return ctx_fail(ctx, PSY_ERR_ARG, "psy_render_batch: at most 65535 renders");
+	cudaSetDevice(ctx->device);
+	std::vector<RenderParams> rps(b->count);
+	std::vector<DevScene> scs(b->count);
+	uint64_t total = 0, pixels = 0;
+	uint32_t max_len = 1, max_spp = 1;
+	unsigned features = 0;
+	int rc;
+	for (uint32_t i = 0; i < b->count; ++i) {
+		psy_ctx* sc = b->scenes[i];
+		if (!sc) return ctx_fail(ctx, PSY_ERR_ARG, "psy_render_batch: render %u has no scene context", i);
+		if (sc->device != ctx->device)
+			return ctx_fail(ctx, PSY_ERR_ARG, "psy_render_batch: render %u's scene is on another device", i);
+		if ((rc = check_render(sc, &b->renders[i], "psy_render_batch")))
+			return ctx_fail(ctx, rc, "render %u: %s", i, sc->last_error.c_str());
+		if (!b->xyz[i]) return ctx_fail(ctx, PSY_ERR_ARG, "psy_render_batch: render %u has no film", i);
+		rps[i] = render_params(sc, &b->renders[i], b->xyz[i], b->counts ? b->counts[i] : nullptr);
+		rps[i].path_base = total;
+		rps[i].pixel_base = pixels;
+		scs[i] = sc->dev;
+		const uint64_t px = (uint64_t)b->renders[i].width * b->renders[i].height;
+		pixels += px;
+		total += px * b->renders[i].spp;
+		if (rps[i].path_length > max_len) max_len = rps[i].path_length;
+		if (rps[i].spp > max_spp) max_spp = rps[i].spp;
+		features |= sc->dev.features;
+	}
+	uint64_t P = b->stream_paths ? b->stream_paths : (ctx->tuned_stream_paths ? ctx->tuned_stream_paths : (1u << 21));
+	if (P > (1ull << 26)) P = 1ull << 26;
+	if (P < max_spp) P = max_spp;
+	if (P > total) P = total;
+	const int block = (int)(b->block_size ? b->block_size : (ctx->tuned_block ? ctx->tuned_block : 128));
+	WaveSet ws;
+	if ((rc = wave_set(ctx, "b_", P, max_len, &ws))) return rc;
+	DevScene* d_scs = static_cast<DevScene*>(ctx->scratch_buffer("b_scenes", sizeof(DevScene) * b->count, &rc));
+	if (!d_scs) return rc;
+	RenderParams* d_rps = static_cast<RenderParams*>(ctx->scratch_buffer("b_renders", sizeof(RenderParams) * b->count, &rc));
+	if (!d_rps) return rc;
+	if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(d_scs, scs.data(), sizeof(DevScene) * b->count, cudaMemcpyHostToDevice, st),
+	                   "psy_render_batch: scene table")))
+		return rc;
+	if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(d_rps, rps.data(), sizeof(RenderParams) * b->count, cudaMemcpyHostToDevice,
+	                                        st),
+	                   "psy_render_batch: render table")))
+		return rc;
+	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, sizeof(unsigned long long), st), "memset"))) return rc;
+	// waves on pixel boundaries
+	std::vector<WaveRange> waves;
+	{
+		uint64_t base = 0, pix = 0;
+		uint32_t r = 0;
+		while (base < total) {
+			uint64_t end = base + P < total ? base + P : total;
+			// the render containing path end - 1, and the end of its last whole pixel
+			while (r + 1 < b->count && rps[r + 1].path_base < end) ++r;
+			uint32_t rr = r;
+			uint64_t local = end - rps[rr].path_base;
+			uint64_t cut = rps[rr].path_base + (local / rps[rr].spp) * rps[rr].spp;
+			if (cut <= base) cut = end;  // cannot happen with P >= max spp
+			end = cut;
+			WaveRange wv;
+			wv.base = base;
+			wv.paths = (int)(end - base);
+			wv.pix_base = pix;
+			// pixels of the wave
+			uint64_t np = 0;
+			for (uint32_t k = 0; k < b->count; ++k) {
+				const uint64_t lo = rps[k].path_base, hi = lo + (uint64_t)rps[k].width * rps[k].height * rps[k].spp;
+				const uint64_t a = base > lo ? base : lo, c = end < hi ? end : hi;
+				if (c > a) np += (c - a) / rps[k].spp;
+			}
+			wv.pixels = (int)np;
+			waves.push_back(wv);
+			pix += np;
+			base = end;
+		}
+	}
+	uint32_t launches = 0;
+	auto launch_all = [&](cudaStream_t s) -> int {
+		for (const WaveRange& wv : waves) {
+			const cudaError_t e = launch_batch_wave(d_scs, d_rps, (int)b->count, features, max_len, ctx->halton, wv,
+			                                        ws.ps, ws.wb, ws.wq, ctx->d_status, block, s, &launches);
+			if (e != cudaSuccess) return ctx_cuda(ctx, e, "psy_render_batch: launch");
+		}
+		return PSY_OK;
+	};
+	if (b->use_graph) {
+		// the graph is valid while the launch parameters are the same
+		std::vector<uint8_t> key;
+		auto put = [&](const void* p, size_t n) {
+			const uint8_t* c = static_cast<const uint8_t*>(p);
+			key.insert(key.end(), c, c + n);
+		};
+		put(&P, sizeof(P));
+		put(&block, sizeof(block));
+		put(&features, sizeof(features));
+		put(&max_len, sizeof(max_len));
+		put(&ws, sizeof(ws));
+		put(&d_scs, sizeof(d_scs));
+		put(&d_rps, sizeof(d_rps));
+		const uint32_t cnt = b->count;
+		put(&cnt, sizeof(cnt));
+		for (const WaveRange& wv : waves) put(&wv, sizeof(wv));
+		if (!ctx->batch_graph || key != ctx->batch_graph_key) {
+			if (ctx->batch_graph) {
+				cudaGraphExecDestroy(ctx->batch_graph);
+				ctx->batch_graph = nullptr;
+			}
+			if (!ctx->capture_stream &&
+			    (rc = ctx_cuda(ctx, cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking),
+			                   "psy_render_batch: stream")))
+				return rc;
+			if ((rc = ctx_cuda(ctx, cudaStreamBeginCapture(ctx->capture_stream, cudaStreamCaptureModeThreadLocal),
+			                   "psy_render_batch: begin capture")))
+				return rc;
+			const int lrc = launch_all(ctx->capture_stream);
+			cudaGraph_t graph = nullptr;
+			const cudaError_t ee = cudaStreamEndCapture(ctx->capture_stream, &graph);
+			if (lrc) {
+				if (graph) cudaGraphDestroy(graph);
+				return lrc;
+			}
+			if ((rc = ctx_cuda(ctx, ee, "psy_render_batch: end capture"))) return rc;
+			const cudaError_t ie = cudaGraphInstantiate(&ctx->batch_graph, graph, 0);
+			cudaGraphDestroy(graph);
+			if ((rc = ctx_cuda(ctx, ie, "psy_render_batch: instantiate"))) {
+				ctx->batch_graph = nullptr;
+				return rc;
+			}
+			ctx->batch_graph_key = key;
+		} else {
+			// the launch count of the captured sequence
+			for (size_t i = 0; i < waves.size(); ++i) launches += 2 + 4 * max_len;
+		}
+		if ((rc = ctx_cuda(ctx, cudaGraphLaunch(ctx->batch_graph, st), "psy_render_batch: graph launch"))) return rc;
+	} else {
+		if ((rc = launch_all(st))) return rc;
+	}
+	if (stats) {
+		unsigned long long rays = 0;
+		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(&rays, ws.wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
+			return rc;
+		if ((rc = ctx->check_status(st))) return rc;
+		stats->paths = total;
+		stats->rays = rays;
+		stats->launches = launches;
+		stats->waves = (uint32_t)waves.size();
+	}
+	return PSY_OK;
+}
+
 extern "C" {
+
 
 const char* psy_version(void) { return PSY_VERSION; }
 
@@ -431,86 +772,104 @@ int psy_light_sample(psy_ctx* ctx, const psy_light_query_soa* q, uint32_t n, con
 int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* counts, psy_render_stats* stats,
                void* stream) {
 	if (!ctx || !desc || !xyz) return PSY_ERR_ARG;
-	if (!ctx->has_scene) return ctx_fail(ctx, PSY_ERR_NO_SCENE, "psy_render: no scene uploaded");
-	if (desc->width == 0 || desc->height == 0 || desc->width > 65535 || desc->height > 65535)
-		return ctx_fail(ctx, PSY_ERR_ARG, "psy_render: resolution must be 1..65535 per axis");
-	if (desc->spp == 0 || desc->spp > 65535) return ctx_fail(ctx, PSY_ERR_ARG, "psy_render: spp must be 1..65535");
-	const uint32_t path_length = desc->path_length ? desc->path_length : 4;
-	if (path_length > 40) return ctx_fail(ctx, PSY_ERR_ARG, "psy_render: path_length must be at most 40");
-	if (ctx->host->assemblies[0].light_root < 0)
-		return ctx_fail(ctx, PSY_ERR_ARG, "psy_render: the scene has no lights (the reference integrator needs one)");
+	int rc = check_render(ctx, desc, "psy_render");
+	if (rc) return rc;
+	return render_single(ctx, desc, render_params(ctx, desc, xyz, counts), false, stats, (cudaStream_t)stream);
+}
+
+int psy_render_diff(psy_ctx* ctx, const psy_render_desc* desc, const psy_diff_desc* diff, float* xyz,
+                    uint32_t* counts, psy_render_stats* stats, void* stream) {
+	if (!ctx || !desc || !diff || !xyz) return PSY_ERR_ARG;
+	int rc = check_render(ctx, desc, "psy_render_diff");
+	if (rc) return rc;
+	RenderParams rp = render_params(ctx, desc, xyz, counts);
+	if ((rc = diff_params(ctx, diff, "psy_render_diff", &rp))) return rc;
+	return render_single(ctx, desc, rp, false, stats, (cudaStream_t)stream);
+}
+
+int psy_render_adjoint(psy_ctx* ctx, const psy_render_desc* desc, const psy_diff_desc* diff, const float* dl_dxyz,
+                       float* grad, psy_render_stats* stats, void* stream) {
+	if (!ctx || !desc || !diff || !dl_dxyz || !grad) return PSY_ERR_ARG;
+	int rc = check_render(ctx, desc, "psy_render_adjoint");
+	if (rc) return rc;
+	if ((desc->path_length ? desc->path_length : 4) > PSY_ADJOINT_MAX_PATH)
+		return ctx_fail(ctx, PSY_ERR_ARG, "psy_render_adjoint: path_length must be at most %d", PSY_ADJOINT_MAX_PATH);
+	// the replay renders into a scratch film: only the gradient is kept
+	const size_t npx = (size_t)desc->width * desc->height;
+	float* film = static_cast<float*>(ctx->scratch_buffer("a_film", npx * 3 * sizeof(float), &rc));
+	if (!film) return rc;
+	RenderParams rp = render_params(ctx, desc, film, nullptr);
+	if ((rc = diff_params(ctx, diff, "psy_render_adjoint", &rp))) return rc;
+	rp.dl_dxyz = dl_dxyz;
+	rp.grad = grad;
+	rp.grad_in_smem = (size_t)rp.param_count * sizeof(float) <= 32768 ? 1 : 0;
+	return render_single(ctx, desc, rp, true, stats, (cudaStream_t)stream);
+}
+
+int psy_render_batch(psy_ctx* ctx, const psy_batch_desc* b, psy_render_stats* stats, void* stream) {
+	if (!ctx || !b) return PSY_ERR_ARG;
+	return render_batch(ctx, b, stats, (cudaStream_t)stream);
+}
+
+int psy_batch_autotune(psy_ctx* ctx, const psy_batch_desc* b, uint32_t spp_divisor, psy_batch_tuning* out) {
+	if (!ctx || !b || !out) return PSY_ERR_ARG;
+	if (b->count == 0 || !b->scenes || !b->renders)
+		return ctx_fail(ctx, PSY_ERR_ARG, "psy_batch_autotune: empty batch");
 	cudaSetDevice(ctx->device);
-	cudaStream_t st = (cudaStream_t)stream;
-	const uint64_t total = (uint64_t)desc->width * desc->height * desc->spp;
-	uint64_t want = desc->stream_paths ? desc->stream_paths : (1ull << 21);
-	if (want > (1ull << 26)) want = 1ull << 26;
-	uint64_t P = (want / desc->spp) * desc->spp;
-	if (P < desc->spp) P = desc->spp;
-	if (P > total) P = total;
+	if (spp_divisor == 0) spp_divisor = 1;
+	// the tuning batch: the same renders with fewer samples, on scratch films
+	std::vector<psy_render_desc> descs(b->renders, b->renders + b->count);
+	size_t film = 0;
+	std::vector<size_t> offs(b->count);
+	for (uint32_t i = 0; i < b->count; ++i) {
+		descs[i].spp = descs[i].spp / spp_divisor ? descs[i].spp / spp_divisor : 1;
+		offs[i] = film;
+		film += (size_t)descs[i].width * descs[i].height * 3;
+	}
 	int rc;
-	auto buf = [&](const char* name, size_t bytes) -> void* { return ctx->scratch_buffer(name, bytes, &rc); };
-	PathSoA ps;
-	ps.smp = (uint32_t*)buf("r_smp", P * 4);
-	ps.dimstep = (uint32_t*)buf("r_dimstep", P * 4);
-	ps.wl = (float*)buf("r_wl", P * 4);
-	ps.time = (float*)buf("r_time", P * 4);
-	ps.last_pdf = (float*)buf("r_lpdf", P * 4);
-	ps.col = (float4*)buf("r_col", P * 16);
-	ps.fcol = (float4*)buf("r_fcol", P * 16);
-	ps.lcol = (float4*)buf("r_lcol", P * 16);
-	ps.hit = (float*)buf("r_hit", P * 64);
-	ps.pray = (float*)buf("r_pray", P * 64);
-	ps.sample = (float*)buf("r_sample", P * 12);
-	WaveQueues wq;
-	wq.q0 = (int*)buf("r_q0", P * 4);
-	wq.q1 = (int*)buf("r_q1", P * 4);
-	wq.counters = (int*)buf("r_counters", sizeof(int) * render_counter_count(path_length));
-	wq.rays = (unsigned long long*)buf("r_rays", sizeof(unsigned long long));
-	WaveBufs wb;
-	wb.cap = (int)P;
-	wb.ray[0] = (float4*)buf("r_ray0", P * 80);
-	wb.ray[1] = (float4*)buf("r_ray1", P * 80);
-	wb.hit_f = (float4*)buf("r_hitf", P * 16);
-	wb.hit_i = (int4*)buf("r_hiti", P * 48);
-	wb.occl = (uint8_t*)buf("r_occl", P);
-	if (!wb.ray[0] || !wb.ray[1] || !wb.hit_f || !wb.hit_i || !wb.occl) return rc ? rc : PSY_ERR_OOM;
-	if (!ps.smp || !ps.dimstep || !ps.wl || !ps.time || !ps.last_pdf || !ps.col || !ps.fcol || !ps.lcol ||
-	    !ps.hit || !ps.pray || !ps.sample || !wq.q0 || !wq.q1 || !wq.counters || !wq.rays)
-		return rc ? rc : PSY_ERR_OOM;
-	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(wq.rays, 0, sizeof(unsigned long long), st), "memset"))) return rc;
-	RenderParams rp;
-	rp.width = desc->width;
-	rp.height = desc->height;
-	rp.spp = desc->spp;
-	rp.seed = desc->seed;
-	rp.path_length = path_length;
-	rp.light_count = (uint32_t)ctx->host->assemblies[0].light_count;
-	rp.min_x = -1.0f;
-	rp.max_x = 1.0f;
-	rp.max_y = (float)desc->height / (float)desc->width;
-	rp.min_y = -rp.max_y;
-	rp.ident_inv = ctx->ident_inv;
-	uint32_t launches = 0, waves = 0;
-	for (uint64_t base = 0; base < total; base += P) {
-		rp.wave_base = base;
-		rp.wave_paths = (int)((total - base) < P ? (total - base) : P);
-		if ((rc = ctx_cuda(ctx,
-		                   launch_render_wave(ctx->dev, ctx->halton, rp, ps, wb, wq, xyz, counts, ctx->d_status, st,
-		                                      &launches),
-		                   "render launch")))
-			return rc;
-		++waves;
+	float* tfilm = static_cast<float*>(ctx->scratch_buffer("t_film", film * sizeof(float), &rc));
+	if (!tfilm) return rc;
+	std::vector<float*> films(b->count);
+	for (uint32_t i = 0; i < b->count; ++i) films[i] = tfilm + offs[i];
+	psy_batch_desc t = *b;
+	t.renders = descs.data();
+	t.xyz = films.data();
+	t.counts = nullptr;
+	cudaStream_t st = nullptr;
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	const uint32_t blocks[3] = {64, 128, 256};
+	psy_batch_tuning best{};
+	best.ms = -1.0f;
+	uint32_t trials = 0;
+	for (uint32_t lg = 14; lg <= 20 && rc == PSY_OK; ++lg) {
+		for (uint32_t bi = 0; bi < 3; ++bi) {
+			t.stream_paths = 1u << lg;
+			t.block_size = blocks[bi];
+			if (trials == 0 && (rc = render_batch(ctx, &t, nullptr, st))) break;  // warm-up
+			cudaEventRecord(e0, st);
+			if ((rc = render_batch(ctx, &t, nullptr, st))) break;
+			cudaEventRecord(e1, st);
+			if ((rc = ctx_cuda(ctx, cudaEventSynchronize(e1), "psy_batch_autotune: synchronize"))) break;
+			float ms = 0.0f;
+			cudaEventElapsedTime(&ms, e0, e1);
+			++trials;
+			if (best.ms < 0.0f || ms < best.ms) {
+				best.ms = ms;
+				best.stream_paths = t.stream_paths;
+				best.block_size = t.block_size;
+			}
+		}
 	}
-	if (stats) {
-		unsigned long long rays = 0;
-		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(&rays, wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
-			return rc;
-		if ((rc = ctx->check_status(st))) return rc;
-		stats->paths = total;
-		stats->rays = rays;
-		stats->launches = launches;
-		stats->waves = waves;
-	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (rc) return rc;
+	if ((rc = ctx->check_status(st))) return rc;
+	best.trials = trials;
+	ctx->tuned_stream_paths = best.stream_paths;
+	ctx->tuned_block = best.block_size;
+	*out = best;
 	return PSY_OK;
 }
 

@@ -38,6 +38,13 @@ struct psy_ctx {
 	psy::HaltonDev halton{};
 	std::vector<void*> const_allocs;
 	float ident_inv = 1.0f;
+	// batched rendering: the instantiated graph of the last batch and the
+	// launch configuration it was captured for, and the autotuner's choice
+	cudaGraphExec_t batch_graph = nullptr;
+	std::vector<uint8_t> batch_graph_key;
+	cudaStream_t capture_stream = nullptr;
+	uint32_t tuned_stream_paths = 0;
+	uint32_t tuned_block = 0;
 
 	~psy_ctx();
 	void free_scene();

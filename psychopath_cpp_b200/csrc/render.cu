@@ -23,6 +23,12 @@
  * path slot.  Finished paths write their film sample
  * (Color_XYZ(col) * XYZ_NORM_FAC); a per-wave reduction adds each pixel's
  * samples in sample order.
+ *
+ * The same kernels serve two modes.  PlainWave renders one scene and takes
+ * the scene and render parameters as kernel parameters.  BatchWave renders
+ * many scenes at once: a wave covers consecutive global paths of several
+ * renders, each path carries its render index, and scenes and parameters
+ * are read from device arrays.
  */
 #include "kernels.h"
 #include "render_device.cuh"
@@ -41,15 +47,16 @@ __device__ __forceinline__ Spec sp(float4 v) {
 // ---------------------------------------------------------------------
 // Ray planes (5 x float4 per position):
 //   0: o.xyz, time   1: d.xyz, odx.x   2: odx.yz, ody.xy   3: ody.z, ddx.xyz
-//   4: ddy.xyz, flag (1 = no ray: the shadow step found no light sample)
-__device__ __forceinline__ void store_ray(float4* rb, int cap, int i, const WorldRayD& r, float flag) {
+//   4: ddy.xyz, tag = render index << 1 | 1 when there is no ray (the shadow
+//      step found no light sample)
+__device__ __forceinline__ void store_ray(float4* rb, int cap, int i, const WorldRayD& r, int tag) {
 	rb[i] = make_float4(r.o.x, r.o.y, r.o.z, r.time);
 	rb[cap + i] = make_float4(r.d.x, r.d.y, r.d.z, r.odx.x);
 	rb[2 * cap + i] = make_float4(r.odx.y, r.odx.z, r.ody.x, r.ody.y);
 	rb[3 * cap + i] = make_float4(r.ody.z, r.ddx.x, r.ddx.y, r.ddx.z);
-	rb[4 * cap + i] = make_float4(r.ddy.x, r.ddy.y, r.ddy.z, flag);
+	rb[4 * cap + i] = make_float4(r.ddy.x, r.ddy.y, r.ddy.z, __int_as_float(tag));
 }
-__device__ __forceinline__ float load_ray(const float4* rb, int cap, int i, WorldRayD* r) {
+__device__ __forceinline__ int load_ray(const float4* rb, int cap, int i, WorldRayD* r) {
 	const float4 a = rb[i], b = rb[cap + i], c = rb[2 * cap + i], d = rb[3 * cap + i], e = rb[4 * cap + i];
 	r->o = V3(a.x, a.y, a.z);
 	r->time = a.w;
@@ -58,7 +65,7 @@ __device__ __forceinline__ float load_ray(const float4* rb, int cap, int i, Worl
 	r->ody = V3(c.z, c.w, d.x);
 	r->ddx = V3(d.y, d.z, d.w);
 	r->ddy = V3(e.x, e.y, e.z);
-	return e.w;
+	return __float_as_int(e.w);
 }
 
 // Hit planes: 0: t, u, v, max_dim (float4)   1: obj, kind | depth << 8,
@@ -103,6 +110,7 @@ struct StoredHit {
 	float t;
 	float bf;           // 1 when the hit was back-facing
 	float col[3];       // closure colour (Lambert)
+	int pid;            // differentiable renders: the shader's first albedo weight, or -1
 	V3 d, odx, ody, ddx, ddy;  // previous ray
 };
 
@@ -115,6 +123,7 @@ __device__ __forceinline__ void load_hit(const PathSoA& ps, int s, StoredHit* h)
 	h->t = c.y;
 	h->col[0] = c.z; h->col[1] = c.w; h->col[2] = d.x;
 	h->bf = d.y;
+	h->pid = __float_as_int(d.z);
 	const float4* r = reinterpret_cast<const float4*>(ps.pray) + (size_t)s * 4;
 	const float4 e = r[0], f = r[1], gg = r[2], hh = r[3];
 	h->d = V3(e.x, e.y, e.z);
@@ -129,7 +138,7 @@ __device__ __forceinline__ void store_hit(const PathSoA& ps, int s, const Stored
 	g[0] = make_float4(h.p.x, h.p.y, h.p.z, h.n.x);
 	g[1] = make_float4(h.n.y, h.n.z, h.off.x, h.off.y);
 	g[2] = make_float4(h.off.z, h.t, h.col[0], h.col[1]);
-	g[3] = make_float4(h.col[2], h.bf, 0.0f, 0.0f);
+	g[3] = make_float4(h.col[2], h.bf, __int_as_float(h.pid), 0.0f);
 	float4* r = reinterpret_cast<float4*>(ps.pray) + (size_t)s * 4;
 	r[0] = make_float4(h.d.x, h.d.y, h.d.z, h.odx.x);
 	r[1] = make_float4(h.odx.y, h.odx.z, h.ody.x, h.ody.y);
@@ -204,6 +213,108 @@ __device__ __forceinline__ void finish_path(const PathSoA& ps, int slot, const S
 	reinterpret_cast<float3*>(ps.sample)[slot] = o;
 }
 
+// ---------------------------------------------------------------------
+// Wave modes: where a kernel finds the scene and parameters of render r
+// ---------------------------------------------------------------------
+struct PlainWave {
+	static constexpr bool BATCH = false;
+	DevScene sc;
+	RenderParams rp;
+	__device__ __forceinline__ const DevScene& scene(int) const { return sc; }
+	__device__ __forceinline__ const RenderParams& render(int) const { return rp; }
+	__device__ __forceinline__ int render_of_path(uint64_t) const { return 0; }
+	__device__ __forceinline__ int render_of_pixel(uint64_t) const { return 0; }
+};
+
+struct BatchWave {
+	static constexpr bool BATCH = true;
+	const DevScene* scenes;
+	const RenderParams* renders;
+	int count;
+	__device__ __forceinline__ const DevScene& scene(int r) const { return scenes[r]; }
+	__device__ __forceinline__ const RenderParams& render(int r) const { return renders[r]; }
+	// the last render whose first path (pixel) is at or before g
+	__device__ __forceinline__ int render_of_path(uint64_t g) const {
+		int lo = 0, hi = count - 1;
+		while (lo < hi) {
+			const int mid = (lo + hi + 1) >> 1;
+			if (renders[mid].path_base <= g) lo = mid; else hi = mid - 1;
+		}
+		return lo;
+	}
+	__device__ __forceinline__ int render_of_pixel(uint64_t q) const {
+		int lo = 0, hi = count - 1;
+		while (lo < hi) {
+			const int mid = (lo + hi + 1) >> 1;
+			if (renders[mid].pixel_base <= q) lo = mid; else hi = mid - 1;
+		}
+		return lo;
+	}
+};
+
+// ---------------------------------------------------------------------
+// Differentiable rendering (no reference counterpart)
+// ---------------------------------------------------------------------
+// Emission scale parameter of object `obj`, or -1.
+__device__ __forceinline__ int emission_param(const RenderParams& rp, int obj) {
+	return (rp.params && obj >= 0) ? rp.object_param[obj] : -1;
+}
+
+// lambert_eval with the albedo taken from parameters when the stored hit's
+// shader has them.
+__device__ __forceinline__ Spec lambert_eval_p(const RenderParams& rp, const StoredHit& sh, V3 out, float wl) {
+	if (sh.pid < 0) return lambert_eval(sh.col, sh.d, out, sh.n, wl);
+	const float c = lambert_cos(sh.d, out, sh.n);
+	const Spec a = albedo_spec(rp.params + sh.pid, wl);
+	Spec f;
+	for (int k = 0; k < 4; ++k) f.e[k] = c * a.e[k];
+	return f;
+}
+
+// Adjoint: adds u . dC/dparams for a radiance contribution C (hero
+// wavelengths) whose albedo factors come from vertices 0..nv-1 of the path
+// and whose emission is scaled by params[lp] (lp < 0: none).  C is a
+// product of the vertices' albedos (linear in their weights) and of the
+// emission scale, so each factor's derivative is C divided by that factor
+// times the factor's own derivative.
+__device__ void grad_add(const RenderParams& rp, float* sg, const PathSoA& ps, int slot, int nv, const Spec& C,
+                         int lp, float wl) {
+	const float4 u4 = ps.adj[slot];
+	const float uc[4] = {u4.x * C.e[0], u4.y * C.e[1], u4.z * C.e[2], u4.w * C.e[3]};
+	float* g = rp.grad_in_smem ? sg : rp.grad;
+	if (lp >= 0) {
+		const float sc = rp.params[lp];
+		if (sc != 0.0f) atomicAdd(g + lp, ((uc[0] + uc[1]) + (uc[2] + uc[3])) / sc);
+	}
+	for (int v = 0; v < nv; ++v) {
+		const int pid = ps.vpid[slot * PSY_ADJ_MAX_VERTS + v];
+		if (pid < 0) continue;
+		const float4 a4 = ps.valb[slot * PSY_ADJ_MAX_VERTS + v];
+		const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+		float q[4];
+		for (int j = 0; j < 4; ++j) q[j] = a[j] != 0.0f ? uc[j] / a[j] : 0.0f;
+		for (int k = 0; k < 4; ++k) {
+			float d = 0.0f;
+			for (int j = 0; j < 4; ++j) d += q[j] * albedo_basis(k, wavelength_n(wl, j));
+			atomicAdd(g + pid + k, d);
+		}
+	}
+}
+
+// Per-block gradient accumulators: cleared at kernel start, added to the
+// global gradient at the end.
+__device__ __forceinline__ void grad_begin(const RenderParams& rp, float* sg) {
+	if (!rp.grad || !rp.grad_in_smem) return;
+	for (int i = threadIdx.x; i < rp.param_count; i += blockDim.x) sg[i] = 0.0f;
+	__syncthreads();
+}
+__device__ __forceinline__ void grad_end(const RenderParams& rp, float* sg) {
+	if (!rp.grad || !rp.grad_in_smem) return;
+	__syncthreads();
+	for (int i = threadIdx.x; i < rp.param_count; i += blockDim.x)
+		if (sg[i] != 0.0f) atomicAdd(rp.grad + i, sg[i]);
+}
+
 // Warp-wide work fetch: lane 0 takes the next 32 queue positions.
 __device__ __forceinline__ int fetch32(int* work) {
 	int base = 0;
@@ -214,15 +325,18 @@ __device__ __forceinline__ int fetch32(int* work) {
 // ---------------------------------------------------------------------
 // Camera rays (next_ray_for_path, step 0: path_trace_integrator.cpp:109-125)
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(128) camera_gen_kernel(DevScene sc, HaltonDev hd, RenderParams rp, PathSoA ps,
-                                                         WaveBufs wb) {
+template <class W>
+__global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, WaveRange wv, PathSoA ps, WaveBufs wb) {
 	const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-	if (slot >= rp.wave_paths) return;
-	const uint64_t gidx = rp.wave_base + (uint64_t)slot;
-	const uint64_t pixel = gidx / rp.spp;
+	if (slot >= wv.paths) return;
+	const uint64_t gidx = wv.base + (uint64_t)slot;
+	const int rid = w.render_of_path(gidx);
+	const RenderParams& rp = w.render(rid);
+	const uint64_t local = gidx - rp.path_base;
+	const uint64_t pixel = local / rp.spp;
 	const uint32_t px = (uint32_t)(pixel % rp.width);
 	const uint32_t py = (uint32_t)(pixel / rp.width);
-	const uint32_t s = (uint32_t)(gidx % rp.spp);
+	const uint32_t s = (uint32_t)(local % rp.spp);
 	const uint32_t smp = sampler_offset(px, py, s, rp.seed);
 	uint32_t dim = 0;
 	const float wl = (sampler_get(hd, smp, dim++) * (WAVELENGTH_MAX - WAVELENGTH_MIN)) + WAVELENGTH_MIN;
@@ -236,8 +350,9 @@ __global__ void __launch_bounds__(128) camera_gen_kernel(DevScene sc, HaltonDev 
 	const float samp_b = sampler_get(hd, smp, dim++);
 	const float samp_c = sampler_get(hd, smp, dim++);
 	WorldRayD wr;
-	camera_ray(sc, rx, ry, dx, dy, samp_c, samp_a, samp_b, &wr);
-	store_ray(wb.ray[0], wb.cap, slot, wr, 0.0f);
+	camera_ray(w.scene(rid), rx, ry, dx, dy, samp_c, samp_a, samp_b, &wr);
+	store_ray(wb.ray[0], wb.cap, slot, wr, rid << 1);
+	if (W::BATCH) ps.rid[slot] = (uint16_t)rid;
 	ps.smp[slot] = smp;
 	ps.dimstep[slot] = dim;  // step 0
 	ps.wl[slot] = wl;
@@ -245,6 +360,16 @@ __global__ void __launch_bounds__(128) camera_gen_kernel(DevScene sc, HaltonDev 
 	ps.last_pdf[slot] = 0.0f;
 	ps.col[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	ps.fcol[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+	if (!W::BATCH && rp.dl_dxyz) {
+		// d(film sum)/d(col) of finish_path: XYZ_NORM_FAC / 4 * CIE(lambda_j)
+		const float* g = rp.dl_dxyz + 3 * pixel;
+		float u[4];
+		for (int j = 0; j < 4; ++j) {
+			const float lw = wavelength_n(wl, j);
+			u[j] = ((g[0] * X_1931(lw) + g[1] * Y_1931(lw)) + g[2] * Z_1931(lw)) * (0.25f * XYZ_NORM_FAC);
+		}
+		ps.adj[slot] = make_float4(u[0], u[1], u[2], u[3]);
+	}
 }
 
 // ---------------------------------------------------------------------
@@ -252,8 +377,8 @@ __global__ void __launch_bounds__(128) camera_gen_kernel(DevScene sc, HaltonDev 
 // ---------------------------------------------------------------------
 // n_dev == nullptr: n_host rays.  OCCL: occlusion rays, the result (1 =
 // blocked or no ray) goes to wb.occl by position.
-template <unsigned F, bool OCCL>
-__global__ void __launch_bounds__(128) trace_wave_kernel(DevScene sc, WaveBufs wb, const float4* __restrict__ rb,
+template <class W, unsigned F, bool OCCL>
+__global__ void __launch_bounds__(256) trace_wave_kernel(W w, WaveBufs wb, const float4* __restrict__ rb,
                                                          const int* n_dev, int n_host, int* work,
                                                          unsigned long long* ray_count, unsigned* status) {
 	const int n = n_dev ? *n_dev : n_host;
@@ -265,13 +390,13 @@ __global__ void __launch_bounds__(128) trace_wave_kernel(DevScene sc, WaveBufs w
 		const int i = base + (threadIdx.x & 31);
 		if (i < n) {
 			WorldRayD wr;
-			const float flag = load_ray(rb, wb.cap, i, &wr);
+			const int tag = load_ray(rb, wb.cap, i, &wr);
 			wr.occl = OCCL;
-			if (OCCL && flag != 0.0f) {
+			if (OCCL && (tag & 1)) {
 				wb.occl[i] = 1;
 			} else {
 				HitRec rec;
-				err |= trace_ray<F>(sc, wr, &rec);
+				err |= trace_ray<F>(w.scene(tag >> 1), wr, &rec);
 				++rays;
 				if (OCCL) wb.occl[i] = rec.obj >= 0 ? 1 : 0;
 				else store_rec(wb, i, rec);
@@ -288,11 +413,12 @@ __global__ void __launch_bounds__(128) trace_wave_kernel(DevScene sc, WaveBufs w
 // (path_trace_integrator.cpp:251-272 and 273-302), then the shadow step of
 // next_ray_for_path (path_trace_integrator.cpp:126-184).
 // ---------------------------------------------------------------------
-template <bool CAMERA, unsigned F>
-__global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev hd, RenderParams rp, PathSoA ps,
-                                                        WaveBufs wb, const int* __restrict__ q_in, const int* n_dev,
-                                                        int n_host, int* q_out, int* n_out, int* work,
-                                                        unsigned* status) {
+template <class W, bool CAMERA, unsigned F>
+__global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathSoA ps, WaveBufs wb,
+                                                        const int* __restrict__ q_in, const int* n_dev, int n_host,
+                                                        int* q_out, int* n_out, int* work, unsigned* status) {
+	extern __shared__ float sgrad[];
+	if (!W::BATCH) grad_begin(w.render(0), sgrad);
 	const int lane = threadIdx.x & 31;
 	const int n = n_dev ? *n_dev : n_host;
 	unsigned err = 0;
@@ -303,9 +429,13 @@ __global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev h
 		bool live = false;
 		int slot = -1;
 		WorldRayD sray;
-		float sflag = 1.0f;
+		int stag = 1;
 		if (i < n) {
 			slot = q_in ? q_in[i] : i;
+			WorldRayD wr;
+			const int rid = load_ray(wb.ray[0], wb.cap, i, &wr) >> 1;
+			const DevScene& sc = w.scene(rid);
+			const RenderParams& rp = w.render(rid);
 			const uint32_t smp = ps.smp[slot];
 			const uint32_t ds = ps.dimstep[slot];
 			uint32_t dim = ds & 0xffffu;
@@ -315,8 +445,6 @@ __global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev h
 			const float last_pdf = ps.last_pdf[slot];
 			Spec col = sp(ps.col[slot]);
 			const Spec fcol = sp(ps.fcol[slot]);
-			WorldRayD wr;
-			load_ray(wb.ray[0], wb.cap, i, &wr);
 			HitRec rec;
 			load_rec(wb, i, &rec);
 			bool done = false;
@@ -325,17 +453,31 @@ __global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev h
 				int closure;
 				float ecol[3], lpdf;
 				make_stored<F>(sc, rec, wr, rp.ident_inv, &sh, &closure, ecol, &lpdf, &err);
+				const int vtx = (int)(step >> 1);  // index of this path vertex
 				if (closure == CLOSURE_EMIT) {
 					done = true;
-					const Spec e = rgb_to_spec(ecol, wl);
+					Spec e = rgb_to_spec(ecol, wl);
+					const int lp = emission_param(rp, rec.obj);
+					if (lp >= 0)
+						for (int k = 0; k < 4; ++k) e.e[k] *= rp.params[lp];
+					Spec C;
 					if (!CAMERA && last_pdf != 0.0f) {
 						const float mis_inv_pdf = power_heuristic(last_pdf, lpdf) / last_pdf;
-						for (int k = 0; k < 4; ++k) col.e[k] += ((fcol.e[k] * last_pdf) * e.e[k]) * mis_inv_pdf;
+						for (int k = 0; k < 4; ++k) C.e[k] = ((fcol.e[k] * last_pdf) * e.e[k]) * mis_inv_pdf;
 					} else {
-						for (int k = 0; k < 4; ++k) col.e[k] += fcol.e[k] * e.e[k];
+						for (int k = 0; k < 4; ++k) C.e[k] = fcol.e[k] * e.e[k];
 					}
+					for (int k = 0; k < 4; ++k) col.e[k] += C.e[k];
+					if (!W::BATCH && rp.grad) grad_add(rp, sgrad, ps, slot, vtx, C, lp, wl);
 				} else if (closure != CLOSURE_LAMBERT) {
 					done = true;  // closures outside the supported set end the path
+				} else {
+					sh.pid = (rp.params && rec.shader >= 0) ? rp.shader_param[rec.shader] : -1;
+					if (!W::BATCH && rp.grad && vtx < PSY_ADJ_MAX_VERTS) {
+						const Spec a = sh.pid >= 0 ? albedo_spec(rp.params + sh.pid, wl) : Spec{};
+						ps.vpid[slot * PSY_ADJ_MAX_VERTS + vtx] = sh.pid;
+						ps.valb[slot * PSY_ADJ_MAX_VERTS + vtx] = f4(a);
+					}
 				}
 			} else {
 				done = true;
@@ -360,6 +502,7 @@ __global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev h
 				q.time = time;
 				q.has_xform = false;
 				q.id = 0;
+				q.obj = -1;
 				q.selection_pdf = 1.0f;
 				q.light_sample_pdf = 1.0f;
 				light_tree_sample(sc, &q, rp.ident_inv);
@@ -370,6 +513,10 @@ __global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev h
 					const float lc = (float)rp.light_count;
 					Spec lcol;
 					for (int k = 0; k < 4; ++k) lcol.e[k] = ((q.spec.e[k] * mis_inv_pdf) * lc) / q.selection_pdf;
+					const int lp = emission_param(rp, q.obj);
+					if (lp >= 0)
+						for (int k = 0; k < 4; ++k) lcol.e[k] *= rp.params[lp];
+					if (!W::BATCH && rp.grad) ps.nee_param[slot] = lp;
 					sray.o = sh.p + sh.off;
 					sray.d = (q.to_light - sh.off) * 0.9995f;
 					sray.time = time;
@@ -377,15 +524,16 @@ __global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev h
 					propagate_differentials(sh, &sray);
 					// the light's contribution if the shadow ray is not blocked
 					// (update_path, shadow result: path_trace_integrator.cpp:235-249)
-					const Spec fac = lambert_eval(sh.col, sh.d, sray.d, sh.n, wl);
+					const Spec fac = lambert_eval_p(rp, sh, sray.d, wl);
 					Spec c;
 					for (int k = 0; k < 4; ++k) c.e[k] = (fcol.e[k] * lcol.e[k]) * fac.e[k];
 					contrib = f4(c);
-					sflag = 0.0f;
+					stag = rid << 1;
 				} else {
 					err |= ERRF_NOLIGHT;
 					sray.o = V3(0.0f); sray.d = V3(0.0f, 0.0f, 1.0f); sray.time = time;
 					sray.odx = sray.ody = sray.ddx = sray.ddy = V3(0.0f);
+					stag = (rid << 1) | 1;
 				}
 				ps.dimstep[slot] = (dim & 0xffffu) | (step << 16);
 				ps.col[slot] = f4(col);
@@ -402,9 +550,10 @@ __global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev h
 		if (live) {
 			const int j = out_base + __popc(m & ((1u << lane) - 1u));
 			q_out[j] = slot;
-			store_ray(wb.ray[1], wb.cap, j, sray, sflag);
+			store_ray(wb.ray[1], wb.cap, j, sray, stag);
 		}
 	}
+	if (!W::BATCH) grad_end(w.render(0), sgrad);
 	if (err) atomicOr(status, err);
 }
 
@@ -413,8 +562,11 @@ __global__ void __launch_bounds__(128) shade_hit_kernel(DevScene sc, HaltonDev h
 // then the bounce step of next_ray_for_path (path_trace_integrator.cpp:185-223).
 // Paths keep their queue position.
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(128) shade_shadow_kernel(HaltonDev hd, RenderParams rp, PathSoA ps, WaveBufs wb,
+template <class W>
+__global__ void __launch_bounds__(256) shade_shadow_kernel(W w, HaltonDev hd, PathSoA ps, WaveBufs wb,
                                                            const int* __restrict__ q_in, const int* n_dev, int* work) {
+	extern __shared__ float sgrad[];
+	if (!W::BATCH) grad_begin(w.render(0), sgrad);
 	const int n = *n_dev;
 	while (true) {
 		const int base = fetch32(work);
@@ -422,15 +574,18 @@ __global__ void __launch_bounds__(128) shade_shadow_kernel(HaltonDev hd, RenderP
 		const int i = base + (threadIdx.x & 31);
 		if (i >= n) continue;
 		const int slot = q_in[i];
+		const int rid = W::BATCH ? (int)ps.rid[slot] : 0;
 		const uint32_t smp = ps.smp[slot];
 		const uint32_t ds = ps.dimstep[slot];
 		uint32_t dim = ds & 0xffffu;
 		uint32_t step = ds >> 16;
 		const float wl = ps.wl[slot];
 		Spec col = sp(ps.col[slot]);
+		const RenderParams& rp = w.render(rid);
 		if (wb.occl[i] == 0) {
 			const Spec c = sp(ps.lcol[slot]);
 			for (int k = 0; k < 4; ++k) col.e[k] += c.e[k];
+			if (!W::BATCH && rp.grad) grad_add(rp, sgrad, ps, slot, (int)(step >> 1) + 1, c, ps.nee_param[slot], wl);
 		}
 		step++;
 		if (step == rp.path_length * 2) {
@@ -450,7 +605,7 @@ __global__ void __launch_bounds__(128) shade_shadow_kernel(HaltonDev hd, RenderP
 		const V3 dir = cosine_sample_hemisphere(si, sj);
 		float pdf = dir.z * (float)PSY_INV_PI_D;
 		const V3 out = zup_to_vec(dir, nn);
-		const Spec filter = lambert_eval(sh.col, sh.d, out, sh.n, wl);
+		const Spec filter = lambert_eval_p(rp, sh, out, wl);
 		WorldRayD wr;
 		wr.o = sh.p + sh.off;
 		wr.d = out;
@@ -459,22 +614,27 @@ __global__ void __launch_bounds__(128) shade_shadow_kernel(HaltonDev hd, RenderP
 		propagate_differentials(sh, &wr);
 		if (pdf < 0.00001f) pdf = 0.00001f;
 		for (int k = 0; k < 4; ++k) fcol.e[k] *= filter.e[k] / pdf;
-		store_ray(wb.ray[0], wb.cap, i, wr, 0.0f);
+		store_ray(wb.ray[0], wb.cap, i, wr, rid << 1);
 		ps.dimstep[slot] = (dim & 0xffffu) | (step << 16);
 		ps.col[slot] = f4(col);
 		ps.fcol[slot] = f4(fcol);
 		ps.last_pdf[slot] = pdf;
 	}
+	if (!W::BATCH) grad_end(w.render(0), sgrad);
 }
 
-// Adds each pixel's samples, in sample order, to the film; rejects
+// Adds each pixel's samples, in sample order, to its render's film; rejects
 // non-finite samples as Film::add_sample does (film/film.hpp:135-153).
-__global__ void film_reduce_kernel(RenderParams rp, PathSoA ps, float* xyz, uint32_t* counts) {
+template <class W>
+__global__ void film_reduce_kernel(W w, WaveRange wv, PathSoA ps) {
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
-	const int npix = rp.wave_paths / rp.spp;
-	if (p >= npix) return;
-	const uint64_t pixel = rp.wave_base / rp.spp + (uint64_t)p;
-	const float3* s = reinterpret_cast<const float3*>(ps.sample) + (size_t)p * rp.spp;
+	if (p >= wv.pixels) return;
+	const uint64_t q = wv.pix_base + (uint64_t)p;
+	const RenderParams& rp = w.render(w.render_of_pixel(q));
+	const uint64_t pixel = q - rp.pixel_base;
+	const uint64_t first = rp.path_base + pixel * rp.spp - wv.base;  // slot of the pixel's first sample
+	const float3* s = reinterpret_cast<const float3*>(ps.sample) + first;
+	float* xyz = rp.xyz;
 	float ax = xyz[pixel * 3], ay = xyz[pixel * 3 + 1], az = xyz[pixel * 3 + 2];
 	uint32_t c = 0;
 	for (uint32_t k = 0; k < rp.spp; ++k) {
@@ -488,83 +648,118 @@ __global__ void film_reduce_kernel(RenderParams rp, PathSoA ps, float* xyz, uint
 	xyz[pixel * 3] = ax;
 	xyz[pixel * 3 + 1] = ay;
 	xyz[pixel * 3 + 2] = az;
-	if (counts) counts[pixel] += c;
+	if (rp.counts) rp.counts[pixel] += c;
 }
 
 // ---------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------
+// Persistent grid: resident blocks of `kernel` at `block` threads x SMs.
 template <typename K>
-static int resident_blocks(K kernel) {
-	int b = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 128, 0);
-	return b < 1 ? 1 : b;
+static int persistent_grid(K kernel, int block) {
+	int dev = 0, sms = 0, b = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, block, 0);
+	return sms * (b < 1 ? 1 : b);
 }
 
 struct WaveGrids {
+	int block = 0;
 	int trace_c, trace_o, shade_c, shade_b, shadow;
 };
 
-template <unsigned F>
-static WaveGrids grids_for() {
-	int dev = 0, sms = 0;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	WaveGrids g;
-	g.trace_c = sms * resident_blocks(trace_wave_kernel<F, false>);
-	g.trace_o = sms * resident_blocks(trace_wave_kernel<F, true>);
-	g.shade_c = sms * resident_blocks(shade_hit_kernel<true, F>);
-	g.shade_b = sms * resident_blocks(shade_hit_kernel<false, F>);
-	g.shadow = sms * resident_blocks(shade_shadow_kernel);
-	return g;
+template <class W, unsigned F>
+static const WaveGrids& grids_for(int block) {
+	// one entry per block size, filled on first use (block sizes 64..256)
+	static WaveGrids g[5];
+	const int k = block == 64 ? 0 : block == 128 ? 1 : block == 256 ? 2 : 3;
+	if (g[k].block != block) {
+		WaveGrids n;
+		n.block = block;
+		n.trace_c = persistent_grid(trace_wave_kernel<W, F, false>, block);
+		n.trace_o = persistent_grid(trace_wave_kernel<W, F, true>, block);
+		n.shade_c = persistent_grid(shade_hit_kernel<W, true, F>, block);
+		n.shade_b = persistent_grid(shade_hit_kernel<W, false, F>, block);
+		n.shadow = persistent_grid(shade_shadow_kernel<W>, block);
+		g[k] = n;
+	}
+	return g[k];
 }
 
-// Counters per wave: [0] camera trace work, [1] camera shade work; per step
-// s >= 1 (shadow and bounce pairs) four more; see launch_wave.
+// Counters per wave: [0] camera trace work, [1] camera shade work, [2]
+// live paths after the camera step; then per bounce eight: [0] shadow trace
+// work, [1] shadow shade work, [2] bounce trace work, [3] bounce shade work,
+// [4] live paths after the bounce.
 int render_counter_count(uint32_t path_length) { return 4 + 8 * (int)path_length; }
 
-template <unsigned F>
-static void launch_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
-                        const WaveBufs& wb, const WaveQueues& wq, unsigned* status, cudaStream_t st,
-                        uint32_t* launches) {
-	static const WaveGrids g = grids_for<F>();
-	const int P = rp.wave_paths;
+template <class W, unsigned F>
+static void launch_wave(const W& w, uint32_t path_length, const HaltonDev& hd, const WaveRange& wv,
+                        const PathSoA& ps, const WaveBufs& wb, const WaveQueues& wq, unsigned* status, int block,
+                        size_t gsmem, cudaStream_t st, uint32_t* launches) {
+	const WaveGrids& g = grids_for<W, F>(block);
+	const int P = wv.paths;
 	int* c = wq.counters;
-	camera_gen_kernel<<<(P + 127) / 128, 128, 0, st>>>(sc, hd, rp, ps, wb);
-	trace_wave_kernel<F, false><<<g.trace_c, 128, 0, st>>>(sc, wb, wb.ray[0], nullptr, P, c + 0, wq.rays, status);
+	cudaMemsetAsync(c, 0, sizeof(int) * render_counter_count(path_length), st);
+	camera_gen_kernel<W><<<(P + block - 1) / block, block, 0, st>>>(w, hd, wv, ps, wb);
+	trace_wave_kernel<W, F, false><<<g.trace_c, block, 0, st>>>(w, wb, wb.ray[0], nullptr, P, c + 0, wq.rays, status);
 	// camera hit -> shadow rays of the live paths into queue 0
 	int* q = wq.q0;
 	int* n = c + 2;
-	shade_hit_kernel<true, F><<<g.shade_c, 128, 0, st>>>(sc, hd, rp, ps, wb, nullptr, nullptr, P, q, n, c + 1, status);
+	shade_hit_kernel<W, true, F><<<g.shade_c, block, gsmem, st>>>(w, hd, ps, wb, nullptr, nullptr, P, q, n, c + 1,
+	                                                             status);
 	*launches += 3;
 	c += 4;
-	for (uint32_t b = 0; b < rp.path_length; ++b) {
-		trace_wave_kernel<F, true><<<g.trace_o, 128, 0, st>>>(sc, wb, wb.ray[1], n, 0, c + 0, wq.rays, status);
-		shade_shadow_kernel<<<g.shadow, 128, 0, st>>>(hd, rp, ps, wb, q, n, c + 1);
+	for (uint32_t b = 0; b < path_length; ++b) {
+		trace_wave_kernel<W, F, true><<<g.trace_o, block, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays, status);
+		shade_shadow_kernel<W><<<g.shadow, block, gsmem, st>>>(w, hd, ps, wb, q, n, c + 1);
 		*launches += 2;
-		if (b + 1 == rp.path_length) break;  // the last shadow step ends every path
-		trace_wave_kernel<F, false><<<g.trace_c, 128, 0, st>>>(sc, wb, wb.ray[0], n, 0, c + 2, wq.rays, status);
+		if (b + 1 == path_length) break;  // the last shadow step ends every path
+		trace_wave_kernel<W, F, false><<<g.trace_c, block, 0, st>>>(w, wb, wb.ray[0], n, 0, c + 2, wq.rays, status);
 		int* q2 = (q == wq.q0) ? wq.q1 : wq.q0;
 		int* n2 = c + 4;
-		shade_hit_kernel<false, F><<<g.shade_b, 128, 0, st>>>(sc, hd, rp, ps, wb, q, n, 0, q2, n2, c + 3, status);
+		shade_hit_kernel<W, false, F><<<g.shade_b, block, gsmem, st>>>(w, hd, ps, wb, q, n, 0, q2, n2, c + 3, status);
 		*launches += 2;
 		q = q2;
 		n = n2;
 		c += 8;
 	}
+	film_reduce_kernel<W><<<(wv.pixels + 127) / 128, 128, 0, st>>>(w, wv, ps);
+	++*launches;
 }
 
-cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const PathSoA& ps,
-                               const WaveBufs& wb, const WaveQueues& wq, float* xyz, uint32_t* counts,
-                               unsigned* status, cudaStream_t st, uint32_t* launches) {
-	cudaMemsetAsync(wq.counters, 0, sizeof(int) * render_counter_count(rp.path_length), st);
+static int valid_block(int block) { return (block == 64 || block == 128 || block == 256) ? block : 128; }
+
+cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const WaveRange& wv,
+                               const PathSoA& ps, const WaveBufs& wb, const WaveQueues& wq, unsigned* status,
+                               int block, cudaStream_t st, uint32_t* launches) {
+	PlainWave w;
+	w.sc = sc;
+	w.rp = rp;
+	block = valid_block(block);
+	const size_t gsmem = (rp.grad && rp.grad_in_smem) ? sizeof(float) * (size_t)rp.param_count : 0;
+	const uint32_t L = rp.path_length;
 	switch (feature_variant(sc.features)) {
-		case FEAT_FLAT: launch_wave<FEAT_FLAT>(sc, hd, rp, ps, wb, wq, status, st, launches); break;
-		case FEAT_STILL: launch_wave<FEAT_STILL>(sc, hd, rp, ps, wb, wq, status, st, launches); break;
-		default: launch_wave<FEAT_ALL>(sc, hd, rp, ps, wb, wq, status, st, launches); break;
+		case FEAT_FLAT: launch_wave<PlainWave, FEAT_FLAT>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches); break;
+		case FEAT_STILL: launch_wave<PlainWave, FEAT_STILL>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches); break;
+		default: launch_wave<PlainWave, FEAT_ALL>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches); break;
 	}
-	film_reduce_kernel<<<(rp.wave_paths / rp.spp + 127) / 128, 128, 0, st>>>(rp, ps, xyz, counts);
-	++*launches;
+	return cudaGetLastError();
+}
+
+cudaError_t launch_batch_wave(const DevScene* scenes, const RenderParams* renders, int count, unsigned features,
+                              uint32_t max_path_length, const HaltonDev& hd, const WaveRange& wv, const PathSoA& ps,
+                              const WaveBufs& wb, const WaveQueues& wq, unsigned* status, int block,
+                              cudaStream_t st, uint32_t* launches) {
+	BatchWave w;
+	w.scenes = scenes;
+	w.renders = renders;
+	w.count = count;
+	block = valid_block(block);
+	if (feature_variant(features) == FEAT_FLAT)
+		launch_wave<BatchWave, FEAT_FLAT>(w, max_path_length, hd, wv, ps, wb, wq, status, block, 0, st, launches);
+	else
+		launch_wave<BatchWave, FEAT_ALL>(w, max_path_length, hd, wv, ps, wb, wq, status, block, 0, st, launches);
 	return cudaGetLastError();
 }
 

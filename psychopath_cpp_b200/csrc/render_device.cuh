@@ -318,6 +318,39 @@ __device__ __forceinline__ Spec lambert_eval(const float* col, V3 in, V3 out, V3
 	return rgb_to_spec(c, wl);
 }
 
+// The cosine factor lambert_eval scales the colour by.
+__device__ __forceinline__ float lambert_cos(V3 in, V3 out, V3 n) {
+	V3 nn = normalized(n);
+	const V3 v = normalized(out);
+	if (dot(nn, in) > 0.0f) nn = nn * -1.0f;
+	const float d = dot(nn, v);
+	return (d > 0.0f ? d : 0.0f) * (float)PSY_INV_PI_D;
+}
+
+// ---------------------------------------------------------------------
+// Parameterised albedo (differentiable rendering; no reference counterpart)
+// ---------------------------------------------------------------------
+// Gaussian basis function k at wavelength w (nm).
+__device__ __forceinline__ float albedo_basis(int k, float w) {
+	const float c = PSY_ALBEDO_BASIS_C0 + (float)k * PSY_ALBEDO_BASIS_STEP;
+	const float x = (w - c) * (1.0f / PSY_ALBEDO_BASIS_SIGMA);
+	return expf(-0.5f * x * x);
+}
+
+// Albedo spectrum at the four hero wavelengths from weights p[0..3].
+__device__ __forceinline__ Spec albedo_spec(const float* p, float hero) {
+	Spec a;
+#pragma unroll
+	for (int i = 0; i < 4; ++i) {
+		const float w = wavelength_n(hero, i);
+		float v = 0.0f;
+#pragma unroll
+		for (int k = 0; k < 4; ++k) v += p[k] * albedo_basis(k, w);
+		a.e[i] = v;
+	}
+	return a;
+}
+
 __device__ __forceinline__ float lambert_pdf(V3 in, V3 out, V3 n) {
 	V3 nn = normalized(n);
 	const V3 v = normalized(out);
@@ -352,6 +385,7 @@ struct LightQuery {
 	M44 xform;
 	bool has_xform;
 	uint64_t id;
+	int obj;              // global object index of the sampled light
 	V3 to_light;
 	Spec spec;
 	float selection_pdf;
@@ -500,6 +534,7 @@ static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, floa
 		if (inst.kind == INST_OBJECT) {
 			const DevObject ob = sc.objects[inst.data];
 			if (ob.kind != OBJ_SPHERE_LIGHT) return;
+			q->obj = inst.data;
 			float p = 1.0f;
 			V3 tl;
 			sphere_light_sample(sc, ob, q->pos, q->u, q->v, q->wavelength, q->time, &tl, &p, &q->spec);

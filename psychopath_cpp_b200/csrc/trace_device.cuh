@@ -34,10 +34,11 @@ struct WorldRayD {
 	bool occl;
 };
 
-// Ray in the current instance space (Ray, basics/ray.hpp:24-37).
+// Ray in the current instance space (Ray, basics/ray.hpp:24-37).  Its
+// width parameters are kept apart (ray_width_of): only patch leaves need
+// them, so they are computed on first use in each space.
 struct LocalRay {
 	V3 o, d, dinv;
-	RayWidth w;
 };
 
 __device__ __forceinline__ M44 load_m44_dev(const float* p) {
@@ -59,7 +60,6 @@ __device__ __forceinline__ LocalRay make_local(const WorldRayD& wr) {
 	LocalRay r;
 	r.o = wr.o;
 	r.d = wr.d;
-	r.w = ray_width_params(r.o, r.d, wr.odx, wr.ody, wr.ddx, wr.ddy);
 	r.dinv = recip3(r.d);
 	return r;
 }
@@ -68,9 +68,15 @@ __device__ __forceinline__ LocalRay make_local_x(const WorldRayD& wr, const M44&
 	LocalRay r;
 	r.o = pos_to(t, wr.o);
 	r.d = dir_to(t, wr.d);
-	r.w = ray_width_params(r.o, r.d, dir_to(t, wr.odx), dir_to(t, wr.ody), dir_to(t, wr.ddx), dir_to(t, wr.ddy));
 	r.dinv = recip3(r.d);
 	return r;
+}
+
+// The width parameters update_ray computes beside the local ray `r` (made
+// from wr with transform t, or none).
+__device__ __forceinline__ RayWidth ray_width_of(const WorldRayD& wr, const LocalRay& r, const M44* t) {
+	if (!t) return ray_width_params(r.o, r.d, wr.odx, wr.ody, wr.ddx, wr.ddy);
+	return ray_width_params(r.o, r.d, dir_to(*t, wr.odx), dir_to(*t, wr.ody), dir_to(*t, wr.ddx), dir_to(*t, wr.ddy));
 }
 
 // Merged motion-transform sequence of a level (the reference's xform_stack frame).
@@ -408,8 +414,8 @@ __device__ __forceinline__ bool patch_node_test(const Patch<NV> (&q)[TSC], float
 // Returns true when a new closest hit was recorded (or, for occlusion rays,
 // when any leaf was hit).
 template <int NV, int TSC>
-__device__ bool patch_intersect(const float* verts, float time, const LocalRay& r, float* max_t, bool occl,
-                                float dice_rate, float min_upoly, PatchHit* hit) {
+__device__ bool patch_intersect(const float* verts, float time, const LocalRay& r, const RayWidth& rw, float* max_t,
+                                bool occl, float dice_rate, float min_upoly, PatchHit* hit) {
 	constexpr int CP = PSY_PATCH_CP_STEP;
 	constexpr int NCP = PSY_PATCH_CP_COUNT;
 	Patch<NV> cur[TSC];
@@ -434,7 +440,7 @@ __device__ bool patch_intersect(const float* verts, float time, const LocalRay& 
 	bool found = false;
 	while (true) {
 		// `cur` is a node whose box the ray hits; max_dim, h0, h1 are its test
-		const float width = smax(ray_min_width(r.w, h0, h1) * dice_rate, min_upoly);
+		const float width = smax(ray_min_width(rw, h0, h1) * dice_rate, min_upoly);
 		bool entered = false;
 		if (max_dim <= width || path.popc() == PSY_SPLIT_STACK - 1 || depth == 127) {
 			const float tt = (h0 + h1) * 0.5f;
@@ -584,6 +590,9 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 	lv[0].inst_base = sc.assemblies[0].inst_base;
 	lvl_frame[0] = -1;
 	LocalRay r = make_local(wr);
+	LocalRay lvr[PSY_MAX_LEVELS];  // ray of each enclosing level, kept while a transformed child is traversed
+	RayWidth rw;                    // width parameters of r, valid when rw_ok
+	bool rw_ok = false;
 	Frame none;
 	none.count = 0;
 
@@ -609,8 +618,8 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 				const bool changed = lvl_frame[L] != lvl_frame[L - 1];
 				--L;
 				if (changed) {
-					if (lvl_frame[L] >= 0) r = make_local_x(wr, frame_at_index_lerp(frames[lvl_frame[L]], wr.time));
-					else r = make_local(wr);
+					r = lvr[L];
+					rw_ok = false;
 				}
 			}
 			if (nsp == 0) break;
@@ -715,7 +724,9 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 						continue;
 					}
 					lvl_frame[L + 1] = L + 1;
+					lvr[L] = r;
 					r = make_local_x(wr, frame_at_index_lerp(frames[L + 1], wr.time));
+					rw_ok = false;
 				} else {
 					lvl_frame[L + 1] = lvl_frame[L];
 				}
@@ -742,16 +753,33 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 
 		// (B) the object instance's test
 		LocalRay lr = r;
-		if (XFORM && inst.xform_count > 0) {
+		M44 om;  // the object's own transform at the ray time
+		const bool oxf = XFORM && inst.xform_count > 0;
+		if (oxf) {
 			const Frame& parent = lvl_frame[L] >= 0 ? frames[lvl_frame[L]] : none;
 			Frame nf;
 			if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &nf)) {
 				err |= ERRF_MOTION;
 				continue;
 			}
-			lr = make_local_x(wr, frame_at_index_lerp(nf, wr.time));
+			om = frame_at_index_lerp(nf, wr.time);
+			lr = make_local_x(wr, om);
 		}
 		const DevObject ob = sc.objects[inst.data];
+		// width parameters for patches: the object's own, or the level's (cached)
+		auto width = [&]() -> RayWidth {
+			if (oxf) return ray_width_of(wr, lr, &om);
+			if (!rw_ok) {
+				if (XFORM && lvl_frame[L] >= 0) {
+					const M44 lm = frame_at_index_lerp(frames[lvl_frame[L]], wr.time);
+					rw = ray_width_of(wr, r, &lm);
+				} else {
+					rw = ray_width_of(wr, r, nullptr);
+				}
+				rw_ok = true;
+			}
+			return rw;
+		};
 		bool hit = false;
 		PatchHit ph;
 		ph.u = ph.v = ph.max_dim = 0.0f;
@@ -772,16 +800,18 @@ __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* r
 			}
 		} else if (ob.kind == OBJ_BILINEAR) {
 			const float* v = sc.fpool + ob.data;
+			const RayWidth w = width();
 			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-				hit = patch_intersect<4, 2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_intersect<4, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
 			else
-				hit = patch_intersect<4, 1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_intersect<4, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
 		} else if ((F & FEAT_BICUBIC) && ob.kind == OBJ_BICUBIC) {
 			const float* v = sc.fpool + ob.data;
+			const RayWidth w = width();
 			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-				hit = patch_intersect<16, 2>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_intersect<16, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
 			else
-				hit = patch_intersect<16, 1>(v, wr.time, lr, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_intersect<16, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
 		}
 		if (hit) {
 			rec->obj = inst.data;

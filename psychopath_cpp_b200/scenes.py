@@ -94,6 +94,23 @@ def plain_scene(seed: int = 1, res=(320, 240), spp: int = 16, n_spheres: int = 6
     return sc
 
 
+def adjoint_scene(seed: int = 1, res=(256, 256), spp: int = 32, n_spheres: int = 64, n_lights: int = 8,
+                  light_power: float = 100.0) -> Scene:
+    """The plain scene's geometry with n_lights sphere lights (total power
+    light_power) spread over a ring above it: the differentiable-render
+    workload (per-sphere albedo basis weights and per-light emission scales)."""
+    sc = plain_scene(seed, res=res, spp=spp, n_spheres=n_spheres)
+    root = sc.root
+    del root.objects["light"]
+    root.instances = [i for i in root.instances if i.data != "light"]
+    for k in range(n_lights):
+        a = 2.0 * math.pi * k / n_lights
+        p = [4.0 * math.cos(a), 4.0 * math.sin(a), 5.5 + 0.5 * math.sin(3 * a)]
+        root.add_object("light%d" % k, SphereLight([p], [0.35], [[light_power / n_lights] * 3]))
+        root.add_instance("light%d" % k)
+    return sc
+
+
 # --------------------------------------------------------------------------
 # Heightfield trace microbenchmark
 # --------------------------------------------------------------------------
