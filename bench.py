@@ -439,12 +439,17 @@ def run_batch_ours(args, rank, local, pg, world):
         torch.cuda.synchronize(dev)
         return s.elapsed_time(e) / steps
 
+    log = lambda *a: print(*a, file=sys.stderr, flush=True)
+    log("batch: %d renders, %d paths per pass" % (len(entries), paths))
     for _ in range(args.warmup):
         plain_pass()
     plain_ms = timed(plain_pass, args.steps)
+    log("batch: plain pass %.1f ms" % plain_ms)
     owner = api.Context(local)
-    b = api.BatchRenderer(owner, entries, use_graph=True)
+    b = api.BatchRenderer(owner, entries, use_graph=False)
     tune = b.autotune(spp_divisor=16)
+    log("batch: tuned %r" % tune)
+    b = api.BatchRenderer(owner, entries, use_graph=True)
     for _ in range(args.warmup):
         b.render(sp, with_stats=False)
     b.render(sp, with_stats=True)

@@ -51,6 +51,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
     objs = []
     cc = nvcc()
     flags = NVCC_FLAGS + list(extra_flags or [])
+    jobs = []
     for src in _sources():
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")
         objs.append(obj)
@@ -62,11 +63,17 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
             cmd += ["-Xptxas", "-v"] if verbose else []
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))
-        if verbose and r.stderr:
-            print(r.stderr)
+        jobs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    # the translation units compile in parallel
+    failed = []
+    for src, proc in jobs:
+        out, err = proc.communicate()
+        if proc.returncode != 0:
+            failed.append("nvcc failed for %s:\n%s\n%s" % (src, out, err))
+        elif verbose and err:
+            print(err)
+    if failed:
+        raise RuntimeError("\n".join(failed))
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         if verbose:

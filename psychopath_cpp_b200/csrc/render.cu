@@ -377,34 +377,62 @@ __global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, Wave
 // ---------------------------------------------------------------------
 // n_dev == nullptr: n_host rays.  OCCL: occlusion rays, the result (1 =
 // blocked or no ray) goes to wb.occl by position.
+//
+// Persistent warps with per-lane ray replacement: a lane whose ray is
+// finished takes the next ray of the queue between traversal steps instead
+// of idling until the slowest ray of its warp is done.
+#define PSY_REFILL_MIN 8  // idle lanes that trigger a refill while rays remain
+
 template <class W, unsigned F, bool OCCL>
 __global__ void __launch_bounds__(256) trace_wave_kernel(W w, WaveBufs wb, const float4* __restrict__ rb,
                                                          const int* n_dev, int n_host, int* work,
                                                          unsigned long long* ray_count, unsigned* status) {
 	const int n = n_dev ? *n_dev : n_host;
+	const int lane = threadIdx.x & 31;
+	const unsigned lt_mask = (1u << lane) - 1u;
 	unsigned err = 0;
 	unsigned long long rays = 0;
+	TraceState<F> st;
+	int my = -1;    // queue position of this lane's ray, -1 = idle
+	int rid = 0;
+	bool more = true;  // the queue may still hold rays (warp-uniform)
 	while (true) {
-		const int base = fetch32(work);
-		if (base >= n) break;
-		const int i = base + (threadIdx.x & 31);
-		if (i < n) {
-			WorldRayD wr;
-			const int tag = load_ray(rb, wb.cap, i, &wr);
-			wr.occl = OCCL;
-			if (OCCL && (tag & 1)) {
-				wb.occl[i] = 1;
-			} else {
-				HitRec rec;
-				err |= trace_ray<F>(w.scene(tag >> 1), wr, &rec);
-				++rays;
-				if (OCCL) wb.occl[i] = rec.obj >= 0 ? 1 : 0;
-				else store_rec(wb, i, rec);
+		const unsigned idle = __ballot_sync(0xffffffffu, my < 0);
+		if (more && (__popc(idle) >= PSY_REFILL_MIN || idle == 0xffffffffu)) {
+			int base = 0;
+			if (lane == 0) base = atomicAdd(work, __popc(idle));
+			base = __shfl_sync(0xffffffffu, base, 0);
+			if (base + __popc(idle) >= n) more = false;
+			if (my < 0) {
+				const int k = base + __popc(idle & lt_mask);
+				if (k < n) {
+					WorldRayD wr;
+					const int tag = load_ray(rb, wb.cap, k, &wr);
+					wr.occl = OCCL;
+					if (OCCL && (tag & 1)) {
+						wb.occl[k] = 1;
+					} else {
+						rid = tag >> 1;
+						trace_init<F>(w.scene(rid), st, wr);
+						my = k;
+						++rays;
+					}
+				}
 			}
+		}
+		if (__ballot_sync(0xffffffffu, my >= 0) == 0u) {
+			if (!more) break;
+			continue;
+		}
+		if (my >= 0 && !trace_step<F>(w.scene(rid), st)) {
+			err |= st.err;
+			if (OCCL) wb.occl[my] = st.rec.obj >= 0 ? 1 : 0;
+			else store_rec(wb, my, st.rec);
+			my = -1;
 		}
 	}
 	for (int o = 16; o > 0; o >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, o);
-	if ((threadIdx.x & 31) == 0 && rays) atomicAdd(ray_count, rays);
+	if (lane == 0 && rays) atomicAdd(ray_count, rays);
 	if (err) atomicOr(status, err);
 }
 

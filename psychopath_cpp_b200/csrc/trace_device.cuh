@@ -382,8 +382,17 @@ __device__ __forceinline__ bool patch_node_test(const Patch<NV> (&q)[TSC], float
 		md = (k == 0) ? ld : smax(md, ld);
 	}
 	*max_dim = md;
-	if (TSC == 1) return box_hit(bb[0], r.o, r.dinv, max_t, h0, h1);
-	return box_hit(box_lerp(t_nalpha, bb[0], bb[TSC - 1]), r.o, r.dinv, max_t, h0, h1);
+	const bool h = (TSC == 1) ? box_hit(bb[0], r.o, r.dinv, max_t, h0, h1)
+	                          : box_hit(box_lerp(t_nalpha, bb[0], bb[TSC - 1]), r.o, r.dinv, max_t, h0, h1);
+	// A NaN far distance comes from 0 * inf: the ray runs exactly along a
+	// box face (a zero direction component, the origin on the face).  The
+	// reference's std::min/max slab test then reports a hit with h0 = 0 and
+	// h1 = NaN, and every sub-box is again NaN or a plain miss, so none of
+	// the subtree's leaves can be taken (their t = (h0 + h1) / 2 is NaN)
+	// while the reference still walks all of it, millions of nodes deep
+	// for a camera ray through the image centre.  Treating it as a miss
+	// gives the same hits.
+	return h && !(*h1 != *h1);
 }
 
 // Sub-patches stored on the current path: one every PSY_PATCH_CP_STEP
@@ -562,273 +571,298 @@ struct Level {
 	int inst_base;
 };
 
-// Traces one ray through the scene. Returns the device error flags.
+// Traversal state of one ray.  trace_init sets it up; each trace_step
+// runs to the next object leaf and tests it, and returns false once the
+// ray is finished (rec and err then hold the result).  Kernels can refill
+// a lane with a new ray between steps.
+template <unsigned F>
+struct TraceState {
+	WorldRayD wr;
+	float max_t;
+	unsigned err;
+	HitRec rec;
+	Level lv[PSY_MAX_LEVELS];
+	Frame frames[PSY_MAX_LEVELS];   // merged frames of transformed levels
+	int lvl_frame[PSY_MAX_LEVELS];  // frame used by each level, -1 = none
+	LocalRay lvr[PSY_MAX_LEVELS];   // ray of each enclosing level, kept while a transformed child is traversed
+	int node_stack[PSY_NODE_STACK];
+	int nsp, L;
+	LocalRay r;                     // the ray in the current level's space
+	RayWidth rw;                    // width parameters of r, valid when rw_ok
+	bool rw_ok;
+};
+
 // F is a mask of FEAT_* scene features; code for absent features is not
 // compiled into the variant, which keeps the flat-scene kernels small.
 template <unsigned F>
-__device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
+__device__ __forceinline__ void trace_init(const DevScene& sc, TraceState<F>& s, const WorldRayD& wr) {
+	s.wr = wr;
+	s.err = 0;
+	s.max_t = wr.occl ? 1.0f : INFINITY;
+	s.rec.obj = -1;
+	s.rec.t = INFINITY;
+	s.rec.depth = 0;
+	s.nsp = 0;
+	s.L = 0;
+	s.lv[0].asmb = 0;
+	s.lv[0].stack_base = 0;
+	s.lv[0].shader = -1;
+	s.lv[0].inst = -1;
+	s.lv[0].id = 0;
+	s.lv[0].id_bits = sc.assemblies[0].id_bits;
+	s.lv[0].inst_base = sc.assemblies[0].inst_base;
+	s.lvl_frame[0] = -1;
+	s.r = make_local(wr);
+	s.rw_ok = false;
+	const int root = sc.assemblies[0].root;
+	if (root != REF_EMPTY) s.node_stack[s.nsp++] = root;
+}
+
+// One step: (A) traverse to the next object leaf, (B) test it.  Running the
+// phases as separate loops lets the lanes of a warp run each phase together.
+// The closest hit does not depend on the order objects are tested in (a
+// sub-patch's box lies inside its parent's, so max_t pruning only drops
+// leaves that could not be closer), except for exact ties.
+template <unsigned F>
+__device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s) {
 	constexpr bool NESTED = (F & FEAT_NESTED) != 0;
 	constexpr bool XFORM = (F & FEAT_XFORM) != 0;
-	unsigned err = 0;
-	float max_t = wr.occl ? 1.0f : INFINITY;
-	rec->obj = -1;
-	rec->t = INFINITY;
-	rec->depth = 0;
-
-	Level lv[PSY_MAX_LEVELS];
-	Frame frames[PSY_MAX_LEVELS];  // merged frames of transformed levels
-	int lvl_frame[PSY_MAX_LEVELS];  // frame used by each level, -1 = none
-	int node_stack[PSY_NODE_STACK];
-	int nsp = 0;
-	int L = 0;
-	lv[0].asmb = 0;
-	lv[0].stack_base = 0;
-	lv[0].shader = -1;
-	lv[0].inst = -1;
-	lv[0].id = 0;
-	lv[0].id_bits = sc.assemblies[0].id_bits;
-	lv[0].inst_base = sc.assemblies[0].inst_base;
-	lvl_frame[0] = -1;
-	LocalRay r = make_local(wr);
-	LocalRay lvr[PSY_MAX_LEVELS];  // ray of each enclosing level, kept while a transformed child is traversed
-	RayWidth rw;                    // width parameters of r, valid when rw_ok
-	bool rw_ok = false;
+	const WorldRayD& wr = s.wr;
 	Frame none;
 	none.count = 0;
-
-	{
-		const int root = sc.assemblies[0].root;
-		if (root != REF_EMPTY) node_stack[nsp++] = root;
-	}
-
-	// The loop alternates two phases so that the lanes of a warp run each
-	// phase together: (A) traverse until the next object leaf, (B) test it.
-	// The closest hit does not depend on the order objects are tested in
-	// (a sub-patch's box lies inside its parent's, so max_t pruning only
-	// drops leaves that could not be closer), except for exact ties.
+	int gi = -1, local = 0, shader = -1;
+	uint64_t id = 0;
+	DevInstance inst;
 	while (true) {
-		int gi = -1, local = 0, shader = -1;
-		uint64_t id = 0;
-		DevInstance inst;
-		bool abort = false;
-		while (true) {
-			gi = -1;
-			// leave finished levels, restoring the ray of the enclosing level
-			while (NESTED && L > 0 && nsp == lv[L].stack_base) {
-				const bool changed = lvl_frame[L] != lvl_frame[L - 1];
-				--L;
-				if (changed) {
-					r = lvr[L];
-					rw_ok = false;
+		// leave finished levels, restoring the ray of the enclosing level
+		while (NESTED && s.L > 0 && s.nsp == s.lv[s.L].stack_base) {
+			const bool changed = s.lvl_frame[s.L] != s.lvl_frame[s.L - 1];
+			--s.L;
+			if (changed) {
+				s.r = s.lvr[s.L];
+				s.rw_ok = false;
+			}
+		}
+		if (s.nsp == 0) return false;
+		const int ref = s.node_stack[--s.nsp];
+		if (ref >= 0) {
+			// inner node: test the child boxes (BBox4::intersect_ray, basics/bbox.hpp:566-595)
+			const DevNode* nd = sc.nodes + ref;
+			float b[24];
+			const float4* q = reinterpret_cast<const float4*>(nd->b);
+#pragma unroll
+			for (int i = 0; i < 6; ++i) {
+				const float4 v = __ldg(q + i);
+				b[i * 4 + 0] = v.x; b[i * 4 + 1] = v.y; b[i * 4 + 2] = v.z; b[i * 4 + 3] = v.w;
+			}
+			const int4 ch = __ldg(reinterpret_cast<const int4*>(nd->child));
+			const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->nchild));
+			const int nch = meta.x;
+			const int ts = meta.y;
+			if (ts > 1) {
+				const SeqPos sp = seq_pos(wr.time, ts);
+				const float* e0 = sp.i0 == 0 ? nd->b : sc.node_extra + (size_t)(meta.z + sp.i0 - 1) * 24;
+				if (sp.single) {
+#pragma unroll
+					for (int i = 0; i < 24; ++i) b[i] = e0[i];
+				} else {
+					const float* e1 = sc.node_extra + (size_t)(meta.z + sp.i0) * 24;
+					const float ia = one_minus(sp.nalpha);
+#pragma unroll
+					for (int i = 0; i < 24; ++i) b[i] = (e0[i] * ia) + (e1[i] * sp.nalpha);
 				}
 			}
-			if (nsp == 0) break;
-			const int ref = node_stack[--nsp];
-			if (ref >= 0) {
-				// inner node: test the child boxes (BBox4::intersect_ray, basics/bbox.hpp:566-595)
-				const DevNode* nd = sc.nodes + ref;
-				float b[24];
-				const float4* q = reinterpret_cast<const float4*>(nd->b);
-	#pragma unroll
-				for (int i = 0; i < 6; ++i) {
-					const float4 v = __ldg(q + i);
-					b[i * 4 + 0] = v.x; b[i * 4 + 1] = v.y; b[i * 4 + 2] = v.z; b[i * 4 + 3] = v.w;
+			// slab tests of the four children; every array index below is a
+			// compile-time constant so the node stays in registers
+			const bool ds0 = s.r.dinv.x < 0.0f, ds1 = s.r.dinv.y < 0.0f, ds2 = s.r.dinv.z < 0.0f;
+			const int chv[4] = {ch.x, ch.y, ch.z, ch.w};
+			float tk[4];
+			int ck[4], sk[4];
+			int nhit = 0;
+#pragma unroll
+			for (int c = 0; c < 4; ++c) {
+				const float x0 = b[0 * 4 + c], x1 = b[1 * 4 + c];
+				const float y0 = b[2 * 4 + c], y1 = b[3 * 4 + c];
+				const float z0 = b[4 * 4 + c], z1 = b[5 * 4 + c];
+				const float xlo = ((ds0 ? x1 : x0) - s.r.o.x) * s.r.dinv.x;
+				const float xhi = ((ds0 ? x0 : x1) - s.r.o.x) * s.r.dinv.x;
+				const float ylo = ((ds1 ? y1 : y0) - s.r.o.y) * s.r.dinv.y;
+				const float yhi = ((ds1 ? y0 : y1) - s.r.o.y) * s.r.dinv.y;
+				const float zlo = ((ds2 ? z1 : z0) - s.r.o.z) * s.r.dinv.z;
+				const float zhi = ((ds2 ? z0 : z1) - s.r.o.z) * s.r.dinv.z;
+				const float mins = vmax(vmax(xlo, ylo), vmax(zlo, 0.0f));
+				const float maxs = vmax(vmin(vmin(xhi, yhi), zhi), -INFINITY) * BBOX_MAXT_ADJUST;
+				const bool h = c < nch && mins < s.max_t && mins <= maxs;
+				// a hit has mins < max_t <= inf, so inf marks the misses
+				tk[c] = h ? mins : INFINITY;
+				ck[c] = chv[c];
+				sk[c] = c;
+				nhit += h ? 1 : 0;
+			}
+			// nearest first, ties in child order (a stable sort by distance)
+			auto cswap = [&](int a, int bb) {
+				if (tk[bb] < tk[a] || (tk[bb] == tk[a] && sk[bb] < sk[a])) {
+					const float t = tk[a]; tk[a] = tk[bb]; tk[bb] = t;
+					const int c = ck[a]; ck[a] = ck[bb]; ck[bb] = c;
+					const int q = sk[a]; sk[a] = sk[bb]; sk[bb] = q;
 				}
-				const int4 ch = __ldg(reinterpret_cast<const int4*>(nd->child));
-				const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->nchild));
-				const int nch = meta.x;
-				const int ts = meta.y;
-				if (ts > 1) {
-					const SeqPos sp = seq_pos(wr.time, ts);
-					const float* e0 = sp.i0 == 0 ? nd->b : sc.node_extra + (size_t)(meta.z + sp.i0 - 1) * 24;
-					if (sp.single) {
-	#pragma unroll
-						for (int i = 0; i < 24; ++i) b[i] = e0[i];
-					} else {
-						const float* e1 = sc.node_extra + (size_t)(meta.z + sp.i0) * 24;
-						const float ia = one_minus(sp.nalpha);
-	#pragma unroll
-						for (int i = 0; i < 24; ++i) b[i] = (e0[i] * ia) + (e1[i] * sp.nalpha);
-					}
-				}
-				// slab tests of the four children; every array index below is a
-				// compile-time constant so the node stays in registers
-				const bool ds0 = r.dinv.x < 0.0f, ds1 = r.dinv.y < 0.0f, ds2 = r.dinv.z < 0.0f;
-				const int chv[4] = {ch.x, ch.y, ch.z, ch.w};
-				float tk[4];
-				int ck[4], sk[4];
-				int nhit = 0;
-	#pragma unroll
-				for (int c = 0; c < 4; ++c) {
-					const float x0 = b[0 * 4 + c], x1 = b[1 * 4 + c];
-					const float y0 = b[2 * 4 + c], y1 = b[3 * 4 + c];
-					const float z0 = b[4 * 4 + c], z1 = b[5 * 4 + c];
-					const float xlo = ((ds0 ? x1 : x0) - r.o.x) * r.dinv.x;
-					const float xhi = ((ds0 ? x0 : x1) - r.o.x) * r.dinv.x;
-					const float ylo = ((ds1 ? y1 : y0) - r.o.y) * r.dinv.y;
-					const float yhi = ((ds1 ? y0 : y1) - r.o.y) * r.dinv.y;
-					const float zlo = ((ds2 ? z1 : z0) - r.o.z) * r.dinv.z;
-					const float zhi = ((ds2 ? z0 : z1) - r.o.z) * r.dinv.z;
-					const float mins = vmax(vmax(xlo, ylo), vmax(zlo, 0.0f));
-					const float maxs = vmax(vmin(vmin(xhi, yhi), zhi), -INFINITY) * BBOX_MAXT_ADJUST;
-					const bool h = c < nch && mins < max_t && mins <= maxs;
-					// a hit has mins < max_t <= inf, so inf marks the misses
-					tk[c] = h ? mins : INFINITY;
-					ck[c] = chv[c];
-					sk[c] = c;
-					nhit += h ? 1 : 0;
-				}
-				// nearest first, ties in child order (a stable sort by distance)
-				auto cswap = [&](int a, int bb) {
-					if (tk[bb] < tk[a] || (tk[bb] == tk[a] && sk[bb] < sk[a])) {
-						const float t = tk[a]; tk[a] = tk[bb]; tk[bb] = t;
-						const int c = ck[a]; ck[a] = ck[bb]; ck[bb] = c;
-						const int q = sk[a]; sk[a] = sk[bb]; sk[bb] = q;
-					}
-				};
-				cswap(0, 1);
-				cswap(2, 3);
-				cswap(0, 2);
-				cswap(1, 3);
-				cswap(1, 2);
-				if (nsp + nhit > PSY_NODE_STACK) {
-					err |= ERRF_STACK;
-					abort = true;
-					break;
-				}
-				if (nhit > 3) node_stack[nsp++] = ck[3];
-				if (nhit > 2) node_stack[nsp++] = ck[2];
-				if (nhit > 1) node_stack[nsp++] = ck[1];
-				if (nhit > 0) node_stack[nsp++] = ck[0];
+			};
+			cswap(0, 1);
+			cswap(2, 3);
+			cswap(0, 2);
+			cswap(1, 3);
+			cswap(1, 2);
+			if (s.nsp + nhit > PSY_NODE_STACK) {
+				s.err |= ERRF_STACK;
+				return false;
+			}
+			if (nhit > 3) s.node_stack[s.nsp++] = ck[3];
+			if (nhit > 2) s.node_stack[s.nsp++] = ck[2];
+			if (nhit > 1) s.node_stack[s.nsp++] = ck[1];
+			if (nhit > 0) s.node_stack[s.nsp++] = ck[0];
+			continue;
+		}
+
+
+		// leaf: one instance of the current level's assembly
+		local = leaf_instance(ref);
+		gi = s.lv[s.L].inst_base + local;
+		inst = sc.instances[gi];
+		id = id_push(s.lv[s.L].id, (uint64_t)local, s.lv[s.L].id_bits);
+		shader = inst.shader >= 0 ? inst.shader : s.lv[s.L].shader;
+
+		if (NESTED && inst.kind == INST_ASSEMBLY) {
+			const int L = s.L;
+			const Frame& parent = s.lvl_frame[L] >= 0 ? s.frames[s.lvl_frame[L]] : none;
+			if (L + 1 >= PSY_MAX_LEVELS) {
+				s.err |= ERRF_LEVELS;
 				continue;
 			}
-
-			// leaf: one instance of the current level's assembly
-			local = leaf_instance(ref);
-			gi = lv[L].inst_base + local;
-			inst = sc.instances[gi];
-			id = id_push(lv[L].id, (uint64_t)local, lv[L].id_bits);
-			shader = inst.shader >= 0 ? inst.shader : lv[L].shader;
-
-			if (NESTED && inst.kind == INST_ASSEMBLY) {
-				const Frame& parent = lvl_frame[L] >= 0 ? frames[lvl_frame[L]] : none;
-				if (L + 1 >= PSY_MAX_LEVELS) {
-					err |= ERRF_LEVELS;
+			const DevAssembly as = sc.assemblies[inst.data];
+			if (as.root == REF_EMPTY) continue;
+			if (XFORM && inst.xform_count > 0) {
+				if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &s.frames[L + 1])) {
+					s.err |= ERRF_MOTION;
 					continue;
 				}
-				const DevAssembly as = sc.assemblies[inst.data];
-				if (as.root == REF_EMPTY) continue;
-				if (XFORM && inst.xform_count > 0) {
-					if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &frames[L + 1])) {
-						err |= ERRF_MOTION;
-						continue;
-					}
-					lvl_frame[L + 1] = L + 1;
-					lvr[L] = r;
-					r = make_local_x(wr, frame_at_index_lerp(frames[L + 1], wr.time));
-					rw_ok = false;
-				} else {
-					lvl_frame[L + 1] = lvl_frame[L];
-				}
-				++L;
-				lv[L].asmb = inst.data;
-				lv[L].stack_base = nsp;
-				lv[L].shader = shader;
-				lv[L].inst = gi;
-				lv[L].id = id;
-				lv[L].id_bits = as.id_bits;
-				lv[L].inst_base = as.inst_base;
-				if (nsp + 1 > PSY_NODE_STACK) {
-					err |= ERRF_STACK;
-					abort = true;
-					break;
-				}
-				node_stack[nsp++] = as.root;
-				gi = -1;
-				continue;
-			}
-			break;  // an object instance
-		}
-		if (abort || gi < 0) break;
-
-		// (B) the object instance's test
-		LocalRay lr = r;
-		M44 om;  // the object's own transform at the ray time
-		const bool oxf = XFORM && inst.xform_count > 0;
-		if (oxf) {
-			const Frame& parent = lvl_frame[L] >= 0 ? frames[lvl_frame[L]] : none;
-			Frame nf;
-			if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &nf)) {
-				err |= ERRF_MOTION;
-				continue;
-			}
-			om = frame_at_index_lerp(nf, wr.time);
-			lr = make_local_x(wr, om);
-		}
-		const DevObject ob = sc.objects[inst.data];
-		// width parameters for patches: the object's own, or the level's (cached)
-		auto width = [&]() -> RayWidth {
-			if (oxf) return ray_width_of(wr, lr, &om);
-			if (!rw_ok) {
-				if (XFORM && lvl_frame[L] >= 0) {
-					const M44 lm = frame_at_index_lerp(frames[lvl_frame[L]], wr.time);
-					rw = ray_width_of(wr, r, &lm);
-				} else {
-					rw = ray_width_of(wr, r, nullptr);
-				}
-				rw_ok = true;
-			}
-			return rw;
-		};
-		bool hit = false;
-		PatchHit ph;
-		ph.u = ph.v = ph.max_dim = 0.0f;
-		if (ob.kind == OBJ_SPHERE || ob.kind == OBJ_SPHERE_LIGHT) {
-			V3 cent;
-			float radi;
-			if (ob.kind == OBJ_SPHERE) {
-				sphere_at(sc, ob, wr.time, &cent, &radi);
+				s.lvl_frame[L + 1] = L + 1;
+				s.lvr[L] = s.r;
+				s.r = make_local_x(wr, frame_at_index_lerp(s.frames[L + 1], wr.time));
+				s.rw_ok = false;
 			} else {
-				float col[3];
-				light_at(sc, ob, wr.time, &cent, &radi, col);
+				s.lvl_frame[L + 1] = s.lvl_frame[L];
 			}
-			const float t = sphere_t(lr.o, lr.d, cent, radi, max_t);
-			if (t >= 0.0f) {
-				hit = true;
-				ph.t = t;
-				if (!wr.occl) max_t = t;
+			s.L = L + 1;
+			Level& nl = s.lv[L + 1];
+			nl.asmb = inst.data;
+			nl.stack_base = s.nsp;
+			nl.shader = shader;
+			nl.inst = gi;
+			nl.id = id;
+			nl.id_bits = as.id_bits;
+			nl.inst_base = as.inst_base;
+			if (s.nsp + 1 > PSY_NODE_STACK) {
+				s.err |= ERRF_STACK;
+				return false;
 			}
-		} else if (ob.kind == OBJ_BILINEAR) {
-			const float* v = sc.fpool + ob.data;
-			const RayWidth w = width();
-			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-				hit = patch_intersect<4, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
-			else
-				hit = patch_intersect<4, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
-		} else if ((F & FEAT_BICUBIC) && ob.kind == OBJ_BICUBIC) {
-			const float* v = sc.fpool + ob.data;
-			const RayWidth w = width();
-			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-				hit = patch_intersect<16, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
-			else
-				hit = patch_intersect<16, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+			s.node_stack[s.nsp++] = as.root;
+			continue;
 		}
-		if (hit) {
-			rec->obj = inst.data;
-			rec->kind = ob.kind;
-			rec->id = id;
-			rec->shader = shader;
-			if (wr.occl) break;
-			rec->t = ph.t;
-			rec->u = ph.u;
-			rec->v = ph.v;
-			rec->max_dim = ph.max_dim;
-			rec->depth = L + 1;
-			for (int k = 1; k <= L; ++k) rec->path[k - 1] = lv[k].inst;
-			rec->path[L] = gi;
-		}
+		break;  // an object instance
 	}
-	return err;
+
+	// (B) the object instance's test
+	const int L = s.L;
+	LocalRay lr = s.r;
+	M44 om;  // the object's own transform at the ray time
+	const bool oxf = XFORM && inst.xform_count > 0;
+	if (oxf) {
+		const Frame& parent = s.lvl_frame[L] >= 0 ? s.frames[s.lvl_frame[L]] : none;
+		Frame nf;
+		if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &nf)) {
+			s.err |= ERRF_MOTION;
+			return true;
+		}
+		om = frame_at_index_lerp(nf, wr.time);
+		lr = make_local_x(wr, om);
+	}
+	const DevObject ob = sc.objects[inst.data];
+	// width parameters for patches: the object's own, or the level's (cached)
+	auto width = [&]() -> RayWidth {
+		if (oxf) return ray_width_of(wr, lr, &om);
+		if (!s.rw_ok) {
+			if (XFORM && s.lvl_frame[L] >= 0) {
+				const M44 lm = frame_at_index_lerp(s.frames[s.lvl_frame[L]], wr.time);
+				s.rw = ray_width_of(wr, s.r, &lm);
+			} else {
+				s.rw = ray_width_of(wr, s.r, nullptr);
+			}
+			s.rw_ok = true;
+		}
+		return s.rw;
+	};
+	bool hit = false;
+	PatchHit ph;
+	ph.u = ph.v = ph.max_dim = 0.0f;
+	float max_t = s.max_t;
+	if (ob.kind == OBJ_SPHERE || ob.kind == OBJ_SPHERE_LIGHT) {
+		V3 cent;
+		float radi;
+		if (ob.kind == OBJ_SPHERE) {
+			sphere_at(sc, ob, wr.time, &cent, &radi);
+		} else {
+			float col[3];
+			light_at(sc, ob, wr.time, &cent, &radi, col);
+		}
+		const float t = sphere_t(lr.o, lr.d, cent, radi, max_t);
+		if (t >= 0.0f) {
+			hit = true;
+			ph.t = t;
+			if (!wr.occl) max_t = t;
+		}
+	} else if (ob.kind == OBJ_BILINEAR) {
+		const float* v = sc.fpool + ob.data;
+		const RayWidth w = width();
+		if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
+			hit = patch_intersect<4, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+		else
+			hit = patch_intersect<4, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+	} else if ((F & FEAT_BICUBIC) && ob.kind == OBJ_BICUBIC) {
+		const float* v = sc.fpool + ob.data;
+		const RayWidth w = width();
+		if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
+			hit = patch_intersect<16, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+		else
+			hit = patch_intersect<16, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+	}
+	s.max_t = max_t;
+	if (hit) {
+		HitRec& rec = s.rec;
+		rec.obj = inst.data;
+		rec.kind = ob.kind;
+		rec.id = id;
+		rec.shader = shader;
+		if (wr.occl) return false;
+		rec.t = ph.t;
+		rec.u = ph.u;
+		rec.v = ph.v;
+		rec.max_dim = ph.max_dim;
+		rec.depth = L + 1;
+		for (int k = 1; k <= L; ++k) rec.path[k - 1] = s.lv[k].inst;
+		rec.path[L] = gi;
+	}
+	return true;
+}
+
+// Traces one ray through the scene. Returns the device error flags.
+template <unsigned F>
+__device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
+	TraceState<F> s;
+	trace_init<F>(sc, s, wr);
+	while (trace_step<F>(sc, s)) {
+	}
+	*rec = s.rec;
+	return s.err;
 }
 
 // Transform from world space into the hit object's space at the ray time
