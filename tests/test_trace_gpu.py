@@ -124,3 +124,28 @@ def test_intersection_fields(ctx, ref_available, which):
     surf = both & (mine["closure"] != 2)
     uv = parity.ulp_diff(out[surf, 1:3], mine["uv"][surf])
     assert uv.size == 0 or np.percentile(uv, 99.9) <= 4
+
+
+def test_rays_along_patch_faces(ctx, ref_available):
+    """Rays that run exactly along a face of the ground patch's sub-boxes (a
+    zero direction component with the origin on the face, e.g. a pinhole
+    camera ray through the image centre column) make the reference's slab
+    test report NaN-distance hits it can never take; the bisection skips
+    those subtrees, with the same results as the reference."""
+    sc = scenes.plain_scene(seed=1)
+    n = 6
+    o = np.array([[0.0, -15.0, 7.0]] * n, np.float32)
+    d = np.array([[0.0, 0.7384976148605347, -0.6742561459541321],
+                  [0.0, 0.60, -0.80], [0.0, 0.70, -0.71], [0.3, 0.0, -0.95], [-0.0, 0.5, -0.866], [0.0, 0.0, -1.0]],
+                 np.float32)
+    o[3] = [2.5, 0.0, 7.0]   # along the y = 0 plane
+    z = np.zeros((n, 3), np.float32)
+    ddx = np.tile(np.array([0.003236, 0.0, 0.0], np.float32), (n, 1))
+    ddy = np.tile(np.array([0.0, 0.0012867, 0.00296925], np.float32), (n, 1))
+    rays = {"o": o, "d": d, "odx": z, "ody": z, "ddx": ddx, "ddy": ddy, "time": np.full(n, 0.25, np.float32),
+            "type": np.ones(n, np.uint16)}
+    ref, mine = _trace_both(ctx, sc, rays)
+    np.testing.assert_array_equal(ref["hit"], mine["hit"])
+    np.testing.assert_array_equal(ref["id"], mine["id"])
+    hit = ref["hit"] != 0
+    np.testing.assert_array_equal(ref["t"][hit], mine["t"][hit])
