@@ -324,16 +324,48 @@ def run_render_ours(args, rank, local, pg, world):
     }
 
 
+def _ref_render_child(q, res, spp, path_length):
+    from psychopath_cpp_b200 import scenes
+    from oracle import psyref
+    ref = psyref.RefScene(scene=scenes.many_light_scene(3, res=res, spp=spp))
+    _, _, rays, secs = ref.render(threads=os.cpu_count() or 1, spp=spp, path_length=path_length, seed=1)
+    q.put((rays, secs))
+
+
+def ref_render_bounded(spp: int, limit_s: float = 240.0):
+    """The reference's render of the frame at `spp` in a child process (spawned,
+    so no CUDA state is inherited) with a time limit: a ray with NaN
+    differentials makes the reference's patch bisection run without end, so a
+    sample that meets one never returns.  Returns (rays, seconds) or None."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_ref_render_child, args=(q, RENDER_RES, spp, RENDER_PATH_LENGTH))
+    p.start()
+    p.join(limit_s)
+    if p.is_alive():
+        p.kill()
+        p.join()
+        return None
+    return q.get() if not q.empty() else None
+
+
 def render_cpu_baseline(spp: int = 4):
     """The reference's PathTraceIntegrator::integrate (oracle/_ref) on this
     host's cores over a bounded sample of the render: the full frame at a
-    few samples per pixel."""
+    few samples per pixel (fewer if the reference does not finish)."""
     from oracle import psyref
     if not psyref.available():
         return None
-    ref = psyref.RefScene(scene=render_workload())
     threads = os.cpu_count() or 1
-    xyz, cnt, rays, secs = ref.render(threads=threads, spp=spp, path_length=RENDER_PATH_LENGTH, seed=1)
+    out = None
+    while spp >= 1 and out is None:
+        out = ref_render_bounded(spp)
+        if out is None:
+            spp //= 2
+    if out is None:
+        return None
+    rays, secs = out
     paths = RENDER_RES[0] * RENDER_RES[1] * spp
     return {"value": round(paths / secs, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
             "mrays_per_s": round(rays / secs / 1e6, 3),
@@ -345,16 +377,18 @@ def run_render_reference(args, spp: int = 2):
     from oracle import psyref
     if not psyref.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libpsyref.so (the reference built from source) is missing"}
-    ref = psyref.RefScene(scene=render_workload())
     threads = os.cpu_count() or 1
     paths = RENDER_RES[0] * RENDER_RES[1] * spp
-    for _ in range(args.warmup):
-        ref.render(threads=threads, spp=spp, path_length=RENDER_PATH_LENGTH, seed=1)
     tot, rays = 0.0, 0
-    for _ in range(args.steps):
-        _, _, r, secs = ref.render(threads=threads, spp=spp, path_length=RENDER_PATH_LENGTH, seed=1)
-        tot += secs
-        rays += r
+    for k in range(args.warmup + args.steps):
+        out = ref_render_bounded(spp)
+        if out is None:
+            return {"impl": "reference", "unavailable": "the reference's render of the frame at %d spp did not finish "
+                                                         "within 240 s (NaN ray differentials stall its patch "
+                                                         "bisection)" % spp}
+        if k >= args.warmup:
+            rays += out[0]
+            tot += out[1]
     ms = tot * 1e3 / args.steps
     value = paths / (ms * 1e-3)
     return {"metric": RENDER_METRIC, "impl": "reference", "value": round(value, 1), "unit": "paths/s", "n_gpus": 0,
@@ -568,7 +602,13 @@ def main():
     ap.add_argument("--stream-paths", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--render-size", default="",
+                    help="WxHxSPP: a smaller frame of the render workload (profiling captures); not a bench line")
     args = ap.parse_args()
+    if args.render_size:
+        global RENDER_RES, RENDER_SPP
+        w, h, spp = (int(x) for x in args.render_size.lower().split("x"))
+        RENDER_RES, RENDER_SPP = (w, h), spp
     args.warmup = max(3, args.warmup)
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":

@@ -449,7 +449,14 @@ __device__ bool patch_intersect(const float* verts, float time, const LocalRay& 
 	bool found = false;
 	while (true) {
 		// `cur` is a node whose box the ray hits; max_dim, h0, h1 are its test
-		const float width = smax(ray_min_width(rw, h0, h1) * dice_rate, min_upoly);
+		// A NaN width (from NaN ray differentials: a grazing hit makes the
+		// next ray's origin differentials 0/0 in transfer_ray_origin_
+		// differential, basics/differential_geometry.hpp:85-98) survives the
+		// reference's std::max, no sub-patch is ever small enough, and its
+		// bisection does not end.  Here it counts as zero width: the leaves
+		// stop at min_upoly, as for a ray with zero differentials.
+		const float wm = ray_min_width(rw, h0, h1) * dice_rate;
+		const float width = (wm != wm) ? min_upoly : smax(wm, min_upoly);
 		bool entered = false;
 		if (max_dim <= width || path.popc() == PSY_SPLIT_STACK - 1 || depth == 127) {
 			const float tt = (h0 + h1) * 0.5f;

@@ -149,3 +149,29 @@ def test_rays_along_patch_faces(ctx, ref_available):
     np.testing.assert_array_equal(ref["id"], mine["id"])
     hit = ref["hit"] != 0
     np.testing.assert_array_equal(ref["t"][hit], mine["t"][hit])
+
+
+def test_nan_differentials_end_at_min_upoly(ctx, ref_available):
+    """A ray whose origin differentials are NaN (the reference makes them
+    0/0 after a grazing hit) has a NaN width; the reference's bisection of a
+    patch then never ends.  Here such a ray is diced like a ray with zero
+    differentials, down to min_upoly_size: the same hits as that ray, which
+    the reference traces normally."""
+    sc = scenes.many_light_scene(3, res=(64, 36), spp=1)
+    o = np.array([[0.5381631851196289, -7.612769603729248, 0.9662054777145386],
+                  [0.7329777479171753, -7.632197856903076, 0.8413196802139282]], np.float32)
+    d = np.array([[0.838919997215271, -0.08366194367408752, -0.5377862453460693],
+                  [-0.17993035912513733, -0.35451218485832214, -0.9175761938095093]], np.float32)
+    n = len(o)
+    nan = np.full((n, 3), np.nan, np.float32)
+    z = np.zeros((n, 3), np.float32)
+    base = {"o": o, "d": d, "time": np.full(n, 0.632986307144165, np.float32), "type": np.full(n, 2, np.uint16)}
+    with_nan = dict(base, odx=nan, ody=nan, ddx=z + 0.1, ddy=z + 0.1)
+    zero = dict(base, odx=z, ody=z, ddx=z, ddy=z)
+    ref, mine_zero = _trace_both(ctx, sc, zero)
+    mine_nan = api.Tracer(ctx).trace(with_nan)
+    np.testing.assert_array_equal(ref["hit"], mine_zero["hit"])
+    np.testing.assert_array_equal(ref["id"], mine_zero["id"])
+    np.testing.assert_array_equal(ref["t"], mine_zero["t"])
+    for k in ("hit", "id", "t", "uv"):
+        np.testing.assert_array_equal(mine_zero[k], mine_nan[k])
