@@ -340,6 +340,7 @@ struct Builder {
 	struct BPrim {
 		size_t instance;
 		V3 c;
+		Box bb;  // bounds over all time samples (surface-area split only)
 	};
 	enum { IS_LEAF = 1 << 0, IS_SKIP = 1 << 8, IS_2ND = 1 << 9, IS_3RD = 1 << 10, IS_4TH = 1 << 11 };
 
@@ -347,9 +348,80 @@ struct Builder {
 		std::vector<BNode> nodes;
 		std::vector<Box> bboxes;
 		std::vector<BPrim> bag;
+		bool sah = false;  // surface-area split (device tree) instead of the reference's midpoint split
 	};
 
+	static float half_area(const Box& b) {
+		const float dx = b.hi.x - b.lo.x, dy = b.hi.y - b.lo.y, dz = b.hi.z - b.lo.z;
+		if (!(dx >= 0.0f && dy >= 0.0f && dz >= 0.0f)) return 0.0f;
+		return dx * dy + dy * dz + dz * dx;
+	}
+
+	// Binned surface-area split (16 bins per axis over the centroid extent).
+	// Returns the last index of the left part, or first - 1 when no bin
+	// boundary separates the primitives (the caller then takes the midpoint
+	// split).
+	size_t sah_split(BVHBuild& b, size_t first, size_t last) {
+		constexpr int NB = 16;
+		V3 mn = b.bag[first].c, mx = b.bag[first].c;
+		for (size_t i = first + 1; i <= last; ++i)
+			for (int d = 0; d < 3; ++d) {
+				const float c = b.bag[i].c[d];
+				mn.at(d) = std::min(mn[d], c);
+				mx.at(d) = std::max(mx[d], c);
+			}
+		auto bin_of = [&](const BPrim& p, int axis) {
+			const float ext = mx[axis] - mn[axis];
+			int k = (int)((p.c[axis] - mn[axis]) / ext * (float)NB);
+			return k < 0 ? 0 : (k >= NB ? NB - 1 : k);
+		};
+		double best = INFINITY;
+		int best_axis = -1, best_bin = -1;
+		for (int axis = 0; axis < 3; ++axis) {
+			if (!(mx[axis] - mn[axis] > 0.0f)) continue;
+			Box bins[NB];
+			size_t cnt[NB] = {0};
+			for (int k = 0; k < NB; ++k) bins[k] = box_empty();
+			for (size_t i = first; i <= last; ++i) {
+				const int k = bin_of(b.bag[i], axis);
+				bins[k] = box_union(bins[k], b.bag[i].bb);
+				++cnt[k];
+			}
+			double right_area[NB];
+			size_t right_cnt[NB];
+			Box acc = box_empty();
+			size_t n = 0;
+			for (int k = NB - 1; k >= 0; --k) {
+				acc = box_union(acc, bins[k]);
+				n += cnt[k];
+				right_area[k] = half_area(acc);
+				right_cnt[k] = n;
+			}
+			acc = box_empty();
+			n = 0;
+			for (int k = 0; k < NB - 1; ++k) {
+				acc = box_union(acc, bins[k]);
+				n += cnt[k];
+				if (n == 0 || right_cnt[k + 1] == 0) continue;
+				const double cost = half_area(acc) * (double)n + right_area[k + 1] * (double)right_cnt[k + 1];
+				if (cost < best) {
+					best = cost;
+					best_axis = axis;
+					best_bin = k;
+				}
+			}
+		}
+		if (best_axis < 0) return first - 1;
+		auto mid = std::partition(b.bag.begin() + first, b.bag.begin() + last + 1,
+		                          [&](const BPrim& p) { return bin_of(p, best_axis) <= best_bin; });
+		return (size_t)(mid - b.bag.begin()) - 1;
+	}
+
 	size_t split_primitives(BVHBuild& b, size_t first, size_t last) {
+		if (b.sah) {
+			const size_t s = sah_split(b, first, last);
+			if (s + 1 > first && s < last) return s;
+		}
 		V3 mn = b.bag[first].c, mx = b.bag[first].c;
 		for (size_t i = first + 1; i <= last; ++i) {
 			for (int d = 0; d < 3; ++d) {
@@ -427,22 +499,31 @@ struct Builder {
 		}
 	};
 
-	// BVH4::build packing (accel/bvh4.cpp:17-159).
-	void build_bvh4(HAssembly& ha, int aidx) {
+	// BVH4::build packing (accel/bvh4.cpp:17-159).  With device == false the
+	// reference's tree (midpoint splits) is built for the reference-form dump
+	// and the assembly's bounds; with device == true a surface-area-split tree
+	// of the same form is built for traversal.  Which valid tree is traversed
+	// does not change a ray's closest hit, only the order candidates are met
+	// (exact ties aside), and the surface-area tree visits fewer nodes.
+	void build_bvh4(HAssembly& ha, int aidx, bool device) {
 		BVHBuild b;
+		b.sah = device;
 		const uint32_t n_inst = ha.d->instance_count;
 		for (uint32_t i = 0; i < n_inst; ++i) {
 			const Box bb = instance_bounds_at(ha, 0.5f, i);
 			BPrim p;
 			p.instance = i;
 			p.c = lerp3(0.5f, bb.lo, bb.hi);
+			p.bb = box_empty();
+			if (device)
+				for (const Box& x : instance_bounds(ha, i)) p.bb = box_union(p.bb, x);
 			b.bag.push_back(p);
 		}
 		RefBVH4& ref = out->ref_bvh4[aidx];
 		DevAssembly& da = out->assemblies[aidx];
-		da.root = REF_EMPTY;
+		if (device) da.root = REF_EMPTY;
 		if (b.bag.empty()) {
-			ha.accel_bounds = {box_empty()};
+			if (!device) ha.accel_bounds = {box_empty()};
 			return;
 		}
 		bvh_recursive(b, ha, 0, 0, b.bag.size() - 1);
@@ -514,10 +595,17 @@ struct Builder {
 			}
 		}
 		recs.pop_back();
-		ha.accel_bounds.assign(b.bboxes.begin() + b.nodes[0].bbox_index,
-		                       b.bboxes.begin() + b.nodes[0].bbox_index + b.nodes[0].ts);
+		if (!device) {
+			ha.accel_bounds.assign(b.bboxes.begin() + b.nodes[0].bbox_index,
+			                       b.bboxes.begin() + b.nodes[0].bbox_index + b.nodes[0].ts);
+			dump_ref(recs, ref);
+			return;
+		}
+		emit_device(recs, da);
+	}
 
-		// reference-form dump
+	// The reference-form record dump (BVH4::Node, accel/bvh4.hpp:39-71).
+	void dump_ref(const std::vector<Rec4>& recs, RefBVH4& ref) {
 		for (const Rec4& r : recs) {
 			float bb[24];
 			std::memcpy(bb, r.b, sizeof(bb));
@@ -527,8 +615,10 @@ struct Builder {
 			ref.ts.push_back(r.ts);
 			ref.data_index.push_back(r.leaf_data ? r.data : 0);
 		}
+	}
 
-		// device nodes: one DevNode per inner record group
+	// Device nodes: one DevNode per inner record group.
+	void emit_device(const std::vector<Rec4>& recs, DevAssembly& da) {
 		std::vector<int> dev_of(recs.size(), -1);
 		for (size_t i = 0; i < recs.size();) {
 			if (recs[i].leaf_data) {
@@ -714,7 +804,8 @@ struct Builder {
 		HAssembly& ha = asms[a];
 		int maxd = depth;
 		for (int c : ha.children) maxd = std::max(maxd, finalize(c, depth + 1));
-		build_bvh4(ha, a);
+		build_bvh4(ha, a, false);
+		build_bvh4(ha, a, true);
 		build_light_tree(ha, a);
 		ha.finalized = true;
 		return maxd;

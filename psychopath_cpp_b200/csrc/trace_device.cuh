@@ -343,6 +343,18 @@ __device__ __forceinline__ void patch_half_v(Patch<16>& p, bool second) {
 	for (int c = 0; c < 4; ++c) bezier_half(p.p[c], p.p[c + 4], p.p[c + 8], p.p[c + 12], second);
 }
 
+// The 24 floats of a BBox4 record (six 128-bit loads).
+__device__ __forceinline__ void load_box4(const float4* q, float* b) {
+#pragma unroll
+	for (int i = 0; i < 6; ++i) {
+		const float4 v = __ldg(q + i);
+		b[i * 4 + 0] = v.x;
+		b[i * 4 + 1] = v.y;
+		b[i * 4 + 2] = v.z;
+		b[i * 4 + 3] = v.w;
+	}
+}
+
 // Path of a node in the bisection tree: one bit per split level.
 struct Bits128 {
 	uint64_t lo, hi;
@@ -656,27 +668,27 @@ __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s)
 			// inner node: test the child boxes (BBox4::intersect_ray, basics/bbox.hpp:566-595)
 			const DevNode* nd = sc.nodes + ref;
 			float b[24];
-			const float4* q = reinterpret_cast<const float4*>(nd->b);
-#pragma unroll
-			for (int i = 0; i < 6; ++i) {
-				const float4 v = __ldg(q + i);
-				b[i * 4 + 0] = v.x; b[i * 4 + 1] = v.y; b[i * 4 + 2] = v.z; b[i * 4 + 3] = v.w;
-			}
+			load_box4(reinterpret_cast<const float4*>(nd->b), b);
 			const int4 ch = __ldg(reinterpret_cast<const int4*>(nd->child));
 			const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->nchild));
 			const int nch = meta.x;
 			const int ts = meta.y;
 			if (ts > 1) {
+				// motion: lerp the boxes of the two time samples around the ray
+				// time (sample 0 is in the node, later ones in node_extra)
 				const SeqPos sp = seq_pos(wr.time, ts);
-				const float* e0 = sp.i0 == 0 ? nd->b : sc.node_extra + (size_t)(meta.z + sp.i0 - 1) * 24;
+				auto extra = [&](int k) {
+					return reinterpret_cast<const float4*>(sc.node_extra + (size_t)(meta.z + k - 1) * 24);
+				};
 				if (sp.single) {
-#pragma unroll
-					for (int i = 0; i < 24; ++i) b[i] = e0[i];
+					if (sp.i0 != 0) load_box4(extra(sp.i0), b);
 				} else {
-					const float* e1 = sc.node_extra + (size_t)(meta.z + sp.i0) * 24;
+					float e1[24];
+					load_box4(extra(sp.i0 + 1), e1);
+					if (sp.i0 != 0) load_box4(extra(sp.i0), b);
 					const float ia = one_minus(sp.nalpha);
 #pragma unroll
-					for (int i = 0; i < 24; ++i) b[i] = (e0[i] * ia) + (e1[i] * sp.nalpha);
+					for (int i = 0; i < 24; ++i) b[i] = (b[i] * ia) + (e1[i] * sp.nalpha);
 				}
 			}
 			// slab tests of the four children; every array index below is a
