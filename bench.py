@@ -596,7 +596,7 @@ def run_adjoint_ours(args, rank, local, pg, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="render", choices=["render", "trace", "batch", "adjoint"])
     ap.add_argument("--stream-paths", type=int, default=0)

@@ -726,15 +726,23 @@ __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s)
 					const int q = sk[a]; sk[a] = sk[bb]; sk[bb] = q;
 				}
 			};
+			if (s.nsp + nhit > PSY_NODE_STACK) {
+				s.err |= ERRF_STACK;
+				return false;
+			}
+			if (wr.occl) {
+				// an occlusion ray stops at any hit, so the order it meets the
+				// children in does not matter: push the hit ones unsorted
+#pragma unroll
+				for (int c = 3; c >= 0; --c)
+					if (tk[c] != INFINITY) s.node_stack[s.nsp++] = ck[c];
+				continue;
+			}
 			cswap(0, 1);
 			cswap(2, 3);
 			cswap(0, 2);
 			cswap(1, 3);
 			cswap(1, 2);
-			if (s.nsp + nhit > PSY_NODE_STACK) {
-				s.err |= ERRF_STACK;
-				return false;
-			}
 			if (nhit > 3) s.node_stack[s.nsp++] = ck[3];
 			if (nhit > 2) s.node_stack[s.nsp++] = ck[2];
 			if (nhit > 1) s.node_stack[s.nsp++] = ck[1];
