@@ -22,6 +22,7 @@ replicas of the workload per rank (the path has no exchange step).
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -36,6 +37,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CLOSEST_RAY = 80  # 60 B read (o, d, t_max, time, ray width, id/flags) + 20 B written (id 8, t, u, v)
+BYTES_PER_OCCLUSION_RAY = 64
+# DRAM bytes per traced ray of the traversal kernel, from the ncu capture in
+# profiles/trace_wave_kernel_many_light_160x90x4.md (dram read + write per
+# launch / rays in that launch)
+TRAFFIC_BYTES_PER_RAY = 300.0
 BYTES_PER_PATH_EXTRA = 20   # sampler seed 4 + pixel 4 + XYZ 12
 RENDER_RES = (1280, 720)
 RENDER_SPP = 64
@@ -266,18 +272,25 @@ def run_render_ours(args, rank, local, pg, world):
         integ.integrate_device(xyz, cnt, sp, with_stats=False)
     integ.integrate_device(xyz, cnt, sp, with_stats=True)  # rays and launches of one render
     rays_per_render = int(integ.stats.rays)
+    occl_per_render = int(integ.stats.occlusion_rays)
     launches_per_render = int(integ.stats.launches)
     paths = w * h * RENDER_SPP
     if pg:
         pg.barrier()
     torch.cuda.synchronize(dev)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the traversal kernels (the dominant ones) are timed by the library with
+    # CUDA events on the render stream around each of their launches
+    ctx.check(ctx.L.psy_profile_enable(ctx.h, 1))
     with ClockSampler(local) as clk:
         start.record(stream)
         for _ in range(args.steps):
             integ.integrate_device(xyz, cnt, sp, with_stats=False)
         end.record(stream)
         torch.cuda.synchronize(dev)
+    trace_ms, trace_launches = C.c_double(), C.c_uint32()
+    ctx.check(ctx.L.psy_profile_read(ctx.h, C.byref(trace_ms), C.byref(trace_launches)))
+    ctx.check(ctx.L.psy_profile_enable(ctx.h, 0))
     ctx.sync(sp)
     if pg:
         pg.barrier()
@@ -286,9 +299,14 @@ def run_render_ours(args, rank, local, pg, world):
     value = world * paths / (ms * 1e-3)
     mrays = world * rays_per_render / (ms * 1e-3) / 1e6
     rbar = rays_per_render / paths
-    bytes_per_path = rbar * BYTES_PER_CLOSEST_RAY + BYTES_PER_PATH_EXTRA
     hbm, peak_kind = measured_peaks()
-    achieved = bytes_per_path * paths / (ms * 1e-3) / 1e9
+    # roofline of the traversal kernels: their algorithmic bytes (80 B per
+    # closest-hit ray, 64 B per occlusion ray) over their own launch time
+    closest = rays_per_render - occl_per_render
+    trace_bytes = (closest * BYTES_PER_CLOSEST_RAY + occl_per_render * BYTES_PER_OCCLUSION_RAY) * args.steps
+    n_trace = max(1, int(trace_launches.value))
+    achieved = trace_bytes / (trace_ms.value * 1e-3) / 1e9 if trace_ms.value > 0 else 0.0
+    traffic = TRAFFIC_BYTES_PER_RAY * rays_per_render * args.steps / n_trace
     # end to end: the public call plus the device->host read of the film each step
     h_xyz = torch.empty(w * h * 3, dtype=torch.float32, pin_memory=True)
     h_cnt = torch.empty(w * h, dtype=torch.int32, pin_memory=True)
@@ -315,8 +333,13 @@ def run_render_ours(args, rank, local, pg, world):
                    "l2": "per-path state (~200 B x 2M paths in flight) larger than L2"},
         "mrays_per_s": round(mrays, 2), "rays_per_path": round(rbar, 4),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 5), "traffic": None, "peak_source": peak_kind,
-                     "basis": "R*80 + 20 B per path (R = rays per path)"},
+                     "frac": round(achieved / hbm, 5), "traffic": round(traffic),
+                     "kernel": "trace_wave_kernel (closest-hit and occlusion traversal)",
+                     "algorithmic_bytes_per_launch": round(trace_bytes / n_trace),
+                     "avg_launch_ms": round(trace_ms.value / n_trace, 4), "launches_timed": n_trace,
+                     "share_of_step": round(trace_ms.value / args.steps / ms, 3), "peak_source": peak_kind,
+                     "basis": "80 B per closest-hit ray, 64 B per occlusion ray; traffic: DRAM bytes per launch "
+                              "scaled from one ncu capture by rays (profiles/)"},
         "e2e": {"value": round(world * paths / (e2e_ms * 1e-3), 1), "unit": "paths/s",
                 "h2d_bytes_per_step": 28, "d2h_bytes_per_step": w * h * 16},
         "gpu_launches": launches_per_render * args.steps,

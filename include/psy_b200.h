@@ -126,9 +126,12 @@ typedef struct psy_scene_desc {
 } psy_scene_desc;
 
 /*
- * Builds the acceleration structures on the host exactly as
- * Assembly::finalize does (BVH with a midpoint split, packed to BVH4; light
- * tree) and uploads the device scene.  Replaces any previous scene.
+ * Builds the acceleration structures on the host as Assembly::finalize does
+ * (BVH with a midpoint split, packed to BVH4, which gives each assembly its
+ * bounds; light tree) and uploads the device scene.  The device walks a
+ * BVH4 of the same form built with surface-area splits: the hits are the
+ * same (exact ties aside), with fewer nodes visited.  Replaces any previous
+ * scene.
  */
 int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* scene);
 
@@ -298,6 +301,7 @@ typedef struct psy_render_stats {
 	uint64_t rays;            /* rays traced (Global::Stats::rays_shot equivalent) */
 	uint32_t launches;        /* kernels launched */
 	uint32_t waves;
+	uint64_t occlusion_rays;  /* of rays, the shadow (occlusion) rays */
 } psy_render_stats;
 
 /*
@@ -309,6 +313,17 @@ typedef struct psy_render_stats {
  */
 int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* counts, psy_render_stats* stats,
                void* stream);
+
+/*
+ * Optional timing of the traversal kernels, for roofline reports (no
+ * counterpart in the reference).  While enabled, psy_render records CUDA
+ * events on its stream around each traversal launch (the first
+ * PSY_PROFILE_MAX_LAUNCHES since the last read); psy_profile_read waits for
+ * them and returns their summed time and count, then starts a new count.
+ */
+#define PSY_PROFILE_MAX_LAUNCHES 4096
+int psy_profile_enable(psy_ctx* ctx, int on);
+int psy_profile_read(psy_ctx* ctx, double* trace_ms, uint32_t* launches);
 
 /* ------------------------------------------------------------------ */
 /* Differentiable rendering: parameters and the path-replay adjoint     */

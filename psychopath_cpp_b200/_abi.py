@@ -110,14 +110,15 @@ class BatchTuning(C.Structure):
 
 
 class RenderStats(C.Structure):
-    _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("launches", C.c_uint32), ("waves", C.c_uint32)]
+    _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("launches", C.c_uint32), ("waves", C.c_uint32),
+                ("occlusion_rays", C.c_uint64)]
 
 
 # every symbol declared in include/psy_b200.h
 EXPORTED = ["psy_ctx_create", "psy_ctx_destroy", "psy_last_error", "psy_version", "psy_scene_upload",
             "psy_scene_stats_get", "psy_build_bvh4", "psy_build_light_tree", "psy_trace", "psy_trace_host", "psy_sync",
             "psy_trace_host_noalloc", "psy_render_batch", "psy_batch_autotune", "psy_render_diff",
-            "psy_render_adjoint",
+            "psy_render_adjoint", "psy_profile_enable", "psy_profile_read",
             "psy_light_sample", "psy_render"]
 
 _lib = None
@@ -143,6 +144,9 @@ def load():
     L.psy_trace.argtypes = [C.c_void_p, C.POINTER(RaySoA), C.c_uint32, C.POINTER(HitSoA), C.c_void_p]
     L.psy_trace_host.argtypes = [C.c_void_p, C.POINTER(RaySoA), C.c_uint32, C.POINTER(HitSoA)]
     L.psy_sync.argtypes = [C.c_void_p, C.c_void_p]
+    if hasattr(L, "psy_profile_enable"):
+        L.psy_profile_enable.argtypes = [C.c_void_p, C.c_int]
+        L.psy_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]
     if hasattr(L, "psy_render_diff"):
         L.psy_render_diff.argtypes = [C.c_void_p, C.POINTER(RenderDesc), C.POINTER(DiffDesc), C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p]

@@ -102,7 +102,15 @@ struct WaveQueues {
 	int* q0;
 	int* q1;
 	int* counters;      // render_counter_count(path_length) work and live counters
-	unsigned long long* rays;
+	unsigned long long* rays;   // [0] closest-hit rays traced, [1] occlusion rays traced
+};
+
+// Optional profiling: CUDA events recorded around each traversal launch, in
+// pairs, on the launch stream (events[2 k], events[2 k + 1] for the k-th).
+struct LaunchTimer {
+	cudaEvent_t* events;
+	int capacity;  // pairs
+	int* used;     // pairs recorded so far
 };
 
 struct LightQuerySoADev {
@@ -118,7 +126,7 @@ int render_counter_count(uint32_t path_length);
 // One wave of a single render: scene and parameters go in kernel parameters.
 cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const WaveRange& wr,
                                const PathSoA& ps, const WaveBufs& wb, const WaveQueues& wq, unsigned* status,
-                               int block, cudaStream_t st, uint32_t* launches);
+                               int block, cudaStream_t st, uint32_t* launches, const LaunchTimer* timer = nullptr);
 
 // One wave of a batch: the render of each path is found in device arrays
 // (scenes and renders, count entries each); features is the union of the

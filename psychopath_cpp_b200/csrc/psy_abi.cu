@@ -44,6 +44,7 @@ psy_ctx::~psy_ctx() {
 	if (d_status) cudaFree(d_status);
 	if (h_status) cudaFreeHost(h_status);
 	if (batch_graph) cudaGraphExecDestroy(batch_graph);
+	for (cudaEvent_t e : timer_events) cudaEventDestroy(e);
 	if (capture_stream) cudaStreamDestroy(capture_stream);
 }
 
@@ -186,7 +187,7 @@ static int wave_set(psy_ctx* ctx, const char* prefix, uint64_t P, uint32_t path_
 	wq.q0 = (int*)buf("q0", P * 4);
 	wq.q1 = (int*)buf("q1", P * 4);
 	wq.counters = (int*)buf("counters", sizeof(int) * render_counter_count(path_length));
-	wq.rays = (unsigned long long*)buf("rays", sizeof(unsigned long long));
+	wq.rays = (unsigned long long*)buf("rays", 2 * sizeof(unsigned long long));
 	WaveBufs& wb = ws->wb;
 	wb.cap = (int)P;
 	wb.ray[0] = (float4*)buf("ray0", P * 80);
@@ -215,7 +216,7 @@ static int render_single(psy_ctx* ctx, const psy_render_desc* desc, const Render
 	if (P > total) P = total;
 	WaveSet ws;
 	if ((rc = wave_set(ctx, "r_", P, rp.path_length, &ws, adjoint))) return rc;
-	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, sizeof(unsigned long long), st), "memset"))) return rc;
+	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, 2 * sizeof(unsigned long long), st), "memset"))) return rc;
 	uint32_t launches = 0, waves = 0;
 	for (uint64_t base = 0; base < total; base += P) {
 		WaveRange wv;
@@ -225,18 +226,20 @@ static int render_single(psy_ctx* ctx, const psy_render_desc* desc, const Render
 		wv.pixels = wv.paths / (int)desc->spp;
 		if ((rc = ctx_cuda(ctx,
 		                   launch_render_wave(ctx->dev, ctx->halton, rp, wv, ws.ps, ws.wb, ws.wq, ctx->d_status,
-		                                      (int)desc->block_size, st, &launches),
+		                                      (int)desc->block_size, st, &launches,
+		                                      ctx->profiling ? &ctx->timer : nullptr),
 		                   "render launch")))
 			return rc;
 		++waves;
 	}
 	if (stats) {
-		unsigned long long rays = 0;
-		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(&rays, ws.wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
+		unsigned long long rays[2] = {0, 0};
+		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(rays, ws.wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
 			return rc;
 		if ((rc = ctx->check_status(st))) return rc;
 		stats->paths = total;
-		stats->rays = rays;
+		stats->rays = rays[0] + rays[1];
+		stats->occlusion_rays = rays[1];
 		stats->launches = launches;
 		stats->waves = waves;
 	}
@@ -334,7 +337,7 @@ static int render_batch(psy_ctx* ctx, const psy_batch_desc* b, psy_render_stats*
 	                                        st),
 	                   "psy_render_batch: render table")))
 		return rc;
-	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, sizeof(unsigned long long), st), "memset"))) return rc;
+	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, 2 * sizeof(unsigned long long), st), "memset"))) return rc;
 	// waves on pixel boundaries
 	std::vector<WaveRange> waves;
 	{
@@ -428,12 +431,13 @@ static int render_batch(psy_ctx* ctx, const psy_batch_desc* b, psy_render_stats*
 		if ((rc = launch_all(st))) return rc;
 	}
 	if (stats) {
-		unsigned long long rays = 0;
-		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(&rays, ws.wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
+		unsigned long long rays[2] = {0, 0};
+		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(rays, ws.wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
 			return rc;
 		if ((rc = ctx->check_status(st))) return rc;
 		stats->paths = total;
-		stats->rays = rays;
+		stats->rays = rays[0] + rays[1];
+		stats->occlusion_rays = rays[1];
 		stats->launches = launches;
 		stats->waves = (uint32_t)waves.size();
 	}
@@ -870,6 +874,43 @@ int psy_batch_autotune(psy_ctx* ctx, const psy_batch_desc* b, uint32_t spp_divis
 	ctx->tuned_stream_paths = best.stream_paths;
 	ctx->tuned_block = best.block_size;
 	*out = best;
+	return PSY_OK;
+}
+
+int psy_profile_enable(psy_ctx* ctx, int on) {
+	if (!ctx) return PSY_ERR_ARG;
+	cudaSetDevice(ctx->device);
+	if (on && ctx->timer_events.empty()) {
+		ctx->timer_events.resize(2 * (size_t)PSY_PROFILE_MAX_LAUNCHES);
+		for (cudaEvent_t& e : ctx->timer_events) {
+			int rc = ctx_cuda(ctx, cudaEventCreate(&e), "psy_profile_enable: event");
+			if (rc) return rc;
+		}
+		ctx->timer.events = ctx->timer_events.data();
+		ctx->timer.capacity = PSY_PROFILE_MAX_LAUNCHES;
+		ctx->timer.used = &ctx->timer_used;
+	}
+	ctx->timer_used = 0;
+	ctx->profiling = on != 0;
+	return PSY_OK;
+}
+
+int psy_profile_read(psy_ctx* ctx, double* trace_ms, uint32_t* launches) {
+	if (!ctx || !trace_ms || !launches) return PSY_ERR_ARG;
+	cudaSetDevice(ctx->device);
+	double ms = 0.0;
+	for (int k = 0; k < ctx->timer_used; ++k) {
+		int rc = ctx_cuda(ctx, cudaEventSynchronize(ctx->timer_events[2 * k + 1]), "psy_profile_read: synchronize");
+		if (rc) return rc;
+		float e = 0.0f;
+		if ((rc = ctx_cuda(ctx, cudaEventElapsedTime(&e, ctx->timer_events[2 * k], ctx->timer_events[2 * k + 1]),
+		                   "psy_profile_read: elapsed")))
+			return rc;
+		ms += e;
+	}
+	*trace_ms = ms;
+	*launches = (uint32_t)ctx->timer_used;
+	ctx->timer_used = 0;
 	return PSY_OK;
 }
 

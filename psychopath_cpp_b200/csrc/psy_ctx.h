@@ -45,6 +45,11 @@ struct psy_ctx {
 	cudaStream_t capture_stream = nullptr;
 	uint32_t tuned_stream_paths = 0;
 	uint32_t tuned_block = 0;
+	// optional timing of the traversal launches (psy_profile_enable)
+	bool profiling = false;
+	std::vector<cudaEvent_t> timer_events;
+	int timer_used = 0;
+	psy::LaunchTimer timer{};
 
 	~psy_ctx();
 	void free_scene();

@@ -727,13 +727,21 @@ int render_counter_count(uint32_t path_length) { return 4 + 8 * (int)path_length
 template <class W, unsigned F>
 static void launch_wave(const W& w, uint32_t path_length, const HaltonDev& hd, const WaveRange& wv,
                         const PathSoA& ps, const WaveBufs& wb, const WaveQueues& wq, unsigned* status, int block,
-                        size_t gsmem, cudaStream_t st, uint32_t* launches) {
+                        size_t gsmem, cudaStream_t st, uint32_t* launches, const LaunchTimer* tm = nullptr) {
 	const WaveGrids& g = grids_for<W, F>(block);
+	auto tstart = [&]() {
+		if (tm && *tm->used < tm->capacity) cudaEventRecord(tm->events[2 * *tm->used], st);
+	};
+	auto tstop = [&]() {
+		if (tm && *tm->used < tm->capacity) cudaEventRecord(tm->events[2 * (*tm->used)++ + 1], st);
+	};
 	const int P = wv.paths;
 	int* c = wq.counters;
 	cudaMemsetAsync(c, 0, sizeof(int) * render_counter_count(path_length), st);
 	camera_gen_kernel<W><<<(P + block - 1) / block, block, 0, st>>>(w, hd, wv, ps, wb);
+	tstart();
 	trace_wave_kernel<W, F, false><<<g.trace_c, block, 0, st>>>(w, wb, wb.ray[0], nullptr, P, c + 0, wq.rays, status);
+	tstop();
 	// camera hit -> shadow rays of the live paths into queue 0
 	int* q = wq.q0;
 	int* n = c + 2;
@@ -742,11 +750,15 @@ static void launch_wave(const W& w, uint32_t path_length, const HaltonDev& hd, c
 	*launches += 3;
 	c += 4;
 	for (uint32_t b = 0; b < path_length; ++b) {
-		trace_wave_kernel<W, F, true><<<g.trace_o, block, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays, status);
+		tstart();
+		trace_wave_kernel<W, F, true><<<g.trace_o, block, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays + 1, status);
+		tstop();
 		shade_shadow_kernel<W><<<g.shadow, block, gsmem, st>>>(w, hd, ps, wb, q, n, c + 1);
 		*launches += 2;
 		if (b + 1 == path_length) break;  // the last shadow step ends every path
+		tstart();
 		trace_wave_kernel<W, F, false><<<g.trace_c, block, 0, st>>>(w, wb, wb.ray[0], n, 0, c + 2, wq.rays, status);
+		tstop();
 		int* q2 = (q == wq.q0) ? wq.q1 : wq.q0;
 		int* n2 = c + 4;
 		shade_hit_kernel<W, false, F><<<g.shade_b, block, gsmem, st>>>(w, hd, ps, wb, q, n, 0, q2, n2, c + 3, status);
@@ -763,7 +775,7 @@ static int valid_block(int block) { return (block == 64 || block == 128 || block
 
 cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const RenderParams& rp, const WaveRange& wv,
                                const PathSoA& ps, const WaveBufs& wb, const WaveQueues& wq, unsigned* status,
-                               int block, cudaStream_t st, uint32_t* launches) {
+                               int block, cudaStream_t st, uint32_t* launches, const LaunchTimer* timer) {
 	PlainWave w;
 	w.sc = sc;
 	w.rp = rp;
@@ -771,9 +783,9 @@ cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const Re
 	const size_t gsmem = (rp.grad && rp.grad_in_smem) ? sizeof(float) * (size_t)rp.param_count : 0;
 	const uint32_t L = rp.path_length;
 	switch (feature_variant(sc.features)) {
-		case FEAT_FLAT: launch_wave<PlainWave, FEAT_FLAT>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches); break;
-		case FEAT_STILL: launch_wave<PlainWave, FEAT_STILL>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches); break;
-		default: launch_wave<PlainWave, FEAT_ALL>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches); break;
+		case FEAT_FLAT: launch_wave<PlainWave, FEAT_FLAT>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches, timer); break;
+		case FEAT_STILL: launch_wave<PlainWave, FEAT_STILL>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches, timer); break;
+		default: launch_wave<PlainWave, FEAT_ALL>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches, timer); break;
 	}
 	return cudaGetLastError();
 }
