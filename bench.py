@@ -39,9 +39,9 @@ sys.path.insert(0, ROOT)
 BYTES_PER_CLOSEST_RAY = 80  # 60 B read (o, d, t_max, time, ray width, id/flags) + 20 B written (id 8, t, u, v)
 BYTES_PER_OCCLUSION_RAY = 64
 # DRAM bytes per traced ray of the traversal kernel, from the ncu capture in
-# profiles/trace_wave_kernel_many_light_160x90x4.md (dram read + write per
-# launch / rays in that launch)
-TRAFFIC_BYTES_PER_RAY = 300.0
+# profiles/trace_wave_kernel_many_light_640x360x4.md (dram read + write of the
+# camera launch / its 921,600 rays)
+TRAFFIC_BYTES_PER_RAY = 1868.0
 BYTES_PER_PATH_EXTRA = 20   # sampler seed 4 + pixel 4 + XYZ 12
 RENDER_RES = (1280, 720)
 RENDER_SPP = 64
