@@ -37,15 +37,19 @@ enum : unsigned {
 	FEAT_XFORM = 2u,         // instance transforms
 	FEAT_BICUBIC = 4u,       // bicubic patches
 	FEAT_PATCH_MOTION = 8u,  // patches with two time samples
-	FEAT_FLAT = 0u,
-	FEAT_STILL = 7u,         // everything but patch motion
-	FEAT_ALL = 15u
+	FEAT_BILINEAR = 16u,     // bilinear patches
+	FEAT_FLAT = 16u,         // spheres, lights and bilinear patches in one level
+	FEAT_STILL_BICUBIC = 7u, // levels, transforms, bicubic patches (no bilinear, no patch motion)
+	FEAT_STILL = 23u,        // everything but patch motion
+	FEAT_ALL = 31u
 };
 
-// The compiled variant (FEAT_FLAT, FEAT_STILL or FEAT_ALL) that covers a
-// scene's features.
+// The compiled variant that covers a scene's features (the smallest of
+// FEAT_FLAT, FEAT_STILL_BICUBIC, FEAT_STILL, FEAT_ALL: smaller variants
+// leave out the code of absent features).
 inline unsigned feature_variant(unsigned f) {
-	if (f == FEAT_FLAT) return FEAT_FLAT;
+	if ((f & ~FEAT_FLAT) == 0u) return FEAT_FLAT;
+	if ((f & ~FEAT_STILL_BICUBIC) == 0u) return FEAT_STILL_BICUBIC;
 	if ((f & ~FEAT_STILL) == 0u) return FEAT_STILL;
 	return FEAT_ALL;
 }

@@ -412,8 +412,10 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 					WorldRayD wr;
 					const int tag = load_ray(rb, wb.cap, k, &wr);
 					wr.occl = OCCL;
-					if (OCCL && (tag & 1)) {
-						wb.occl[k] = 1;
+					if (tag & 1) {
+						// no ray: a shadow step without a light sample, or a
+						// path of a shorter render in a batch that has ended
+						if (OCCL) wb.occl[k] = 1;
 					} else {
 						rid = tag >> 1;
 						trace_init<F>(w.scene(rid), st, wr);
@@ -461,10 +463,13 @@ __global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathS
 		int slot = -1;
 		WorldRayD sray;
 		int stag = 1;
-		if (i < n) {
+		WorldRayD wr;
+		const int tag = i < n ? load_ray(wb.ray[0], wb.cap, i, &wr) : 1;
+		// (tag & 1): the path ended at its own path length before this step
+		// (a shorter render of a batch) and is only waiting in the queue
+		if (i < n && !(tag & 1)) {
 			slot = q_in ? q_in[i] : i;
-			WorldRayD wr;
-			const int rid = load_ray(wb.ray[0], wb.cap, i, &wr) >> 1;
+			const int rid = tag >> 1;
 			const DevScene& sc = w.scene(rid);
 			const RenderParams& rp = w.render(rid);
 			const uint32_t smp = ps.smp[slot];
@@ -621,6 +626,12 @@ __global__ void __launch_bounds__(256) shade_shadow_kernel(W w, HaltonDev hd, Pa
 		step++;
 		if (step == rp.path_length * 2) {
 			finish_path(ps, slot, col, wl);
+			// paths of longer renders in the same batch keep going: leave a
+			// "no ray" mark so later steps pass over this queue position
+			WorldRayD none;
+			none.o = none.d = none.odx = none.ody = none.ddx = none.ddy = V3(0.0f);
+			none.time = 0.0f;
+			store_ray(wb.ray[0], wb.cap, i, none, (rid << 1) | 1);
 			continue;
 		}
 		StoredHit sh;
@@ -784,6 +795,7 @@ cudaError_t launch_render_wave(const DevScene& sc, const HaltonDev& hd, const Re
 	const uint32_t L = rp.path_length;
 	switch (feature_variant(sc.features)) {
 		case FEAT_FLAT: launch_wave<PlainWave, FEAT_FLAT>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches, timer); break;
+		case FEAT_STILL_BICUBIC: launch_wave<PlainWave, FEAT_STILL_BICUBIC>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches, timer); break;
 		case FEAT_STILL: launch_wave<PlainWave, FEAT_STILL>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches, timer); break;
 		default: launch_wave<PlainWave, FEAT_ALL>(w, L, hd, wv, ps, wb, wq, status, block, gsmem, st, launches, timer); break;
 	}

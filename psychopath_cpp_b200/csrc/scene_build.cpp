@@ -851,6 +851,7 @@ struct Builder {
 		}
 		for (const DevObject& ob : out->objects) {
 			if (ob.kind == OBJ_BICUBIC) out->features |= FEAT_BICUBIC;
+			if (ob.kind == OBJ_BILINEAR) out->features |= FEAT_BILINEAR;
 			if ((ob.kind == OBJ_BILINEAR || ob.kind == OBJ_BICUBIC) && ob.n0 > 1) out->features |= FEAT_PATCH_MOTION;
 			if ((ob.kind == OBJ_BILINEAR || ob.kind == OBJ_BICUBIC) && ob.n0 > 2) return fail("patches support at most two time samples");
 		}

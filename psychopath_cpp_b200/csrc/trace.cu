@@ -102,6 +102,7 @@ cudaError_t launch_trace(const DevScene& sc, const RaySoA& rays, const HitSoA& h
 	const uint32_t grid = (n + block - 1) / block;
 	switch (feature_variant(sc.features)) {
 		case FEAT_FLAT: trace_kernel<FEAT_FLAT><<<grid, block, 0, stream>>>(sc, rays, hits, n, status); break;
+		case FEAT_STILL_BICUBIC: trace_kernel<FEAT_STILL_BICUBIC><<<grid, block, 0, stream>>>(sc, rays, hits, n, status); break;
 		case FEAT_STILL: trace_kernel<FEAT_STILL><<<grid, block, 0, stream>>>(sc, rays, hits, n, status); break;
 		default: trace_kernel<FEAT_ALL><<<grid, block, 0, stream>>>(sc, rays, hits, n, status); break;
 	}

@@ -847,7 +847,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s)
 			ph.t = t;
 			if (!wr.occl) max_t = t;
 		}
-	} else if (ob.kind == OBJ_BILINEAR) {
+	} else if ((F & FEAT_BILINEAR) && ob.kind == OBJ_BILINEAR) {
 		const float* v = sc.fpool + ob.data;
 		const RayWidth w = width();
 		if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)

@@ -88,3 +88,26 @@ def test_batch_autotune(batch_scenes):
     for (xyz, cnt), (bx, bc) in zip(_plain(batch_scenes), b.images()):
         np.testing.assert_array_equal(xyz.view(np.uint32), bx.view(np.uint32))
     owner.close()
+
+
+def test_batch_mixing_flat_and_instanced_scenes():
+    """A batch whose scenes need different traversal variants (one flat, one
+    with nested motion-blurred instances and bicubic patches) runs on the
+    variant covering both; every film still equals its plain render."""
+    entries, plain, ctxs = [], [], []
+    specs = [(scenes.batch_scene(9, (40, 30), 6, 300, 3), (40, 30), 6, 4),
+             (scenes.many_light_scene(7, res=(36, 20), spp=4, n_patches=60, n_groups=20, n_lights=200), (36, 20), 4, 6)]
+    for sc, res, spp, L in specs:
+        c = api.Context(0)
+        c.upload(sc)
+        ctxs.append(c)
+        plain.append(api.PathTraceIntegrator(c, res[0], res[1], spp, seed=3, path_length=L).integrate())
+        entries.append({"scene": c, "width": res[0], "height": res[1], "spp": spp, "seed": 3, "path_length": L})
+    owner = api.Context(0)
+    b = api.BatchRenderer(owner, entries, stream_paths=2048, use_graph=False)
+    b.render()
+    for (xyz, cnt), (bx, bc) in zip(plain, b.images()):
+        np.testing.assert_array_equal(cnt, bc)
+        np.testing.assert_array_equal(xyz.view(np.uint32), bx.view(np.uint32))
+    for c in ctxs + [owner]:
+        c.close()
