@@ -384,7 +384,29 @@ __global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, Wave
 // of 256 threads (128 registers a thread) hide more latency than the
 // register-unbounded variant's two blocks of 128 (measured: +13% on the
 // many-light scene, no change on flat scenes).
+#ifndef PSY_REFILL_MIN
 #define PSY_REFILL_MIN 8  // idle lanes that trigger a refill while rays remain
+#endif
+// Each lane's traversal is cut into three kinds of work: node visits (up to
+// PSY_WALK_NODES at a time, stopping at a leaf), leaf visits (entering an
+// assembly instance, testing an object, starting a patch bisection) and
+// bisection iterations (PSY_PATCH_UNITS at a time).  Each loop iteration of
+// a warp runs the kind that most of its lanes have next (leaf visits
+// counted PSY_LEAF_WEIGHT times, bisections PSY_PATCH_WEIGHT times), so
+// that the lanes doing the same work run together instead of one lane's
+// long bisection or transformed-instance entry holding up the others.
+#ifndef PSY_WALK_NODES
+#define PSY_WALK_NODES 8
+#endif
+#ifndef PSY_PATCH_UNITS
+#define PSY_PATCH_UNITS 8
+#endif
+#ifndef PSY_PATCH_WEIGHT
+#define PSY_PATCH_WEIGHT 1
+#endif
+#ifndef PSY_LEAF_WEIGHT
+#define PSY_LEAF_WEIGHT 1
+#endif
 
 template <class W, unsigned F, bool OCCL>
 __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, const float4* __restrict__ rb,
@@ -397,6 +419,7 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 	unsigned long long rays = 0;
 	TraceState<F> st;
 	int my = -1;    // queue position of this lane's ray, -1 = idle
+	bool at_leaf = false;  // walk_nodes stopped at a leaf (st.leaf)
 	int rid = 0;
 	bool more = true;  // the queue may still hold rays (warp-uniform)
 	while (true) {
@@ -420,16 +443,38 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 						rid = tag >> 1;
 						trace_init<F>(w.scene(rid), st, wr);
 						my = k;
+						at_leaf = false;
 						++rays;
 					}
 				}
 			}
 		}
-		if (__ballot_sync(0xffffffffu, my >= 0) == 0u) {
+		// 0 = idle, 1 = node visits, 2 = leaf visit, 3 = bisection
+		const int kind = my < 0 ? 0 : st.pmode != PM_NONE ? 3 : at_leaf ? 2 : 1;
+		const unsigned nmask = __ballot_sync(0xffffffffu, kind == 1);
+		const unsigned lmask = __ballot_sync(0xffffffffu, kind == 2);
+		const unsigned pmask = __ballot_sync(0xffffffffu, kind == 3);
+		if ((nmask | lmask | pmask) == 0u) {
 			if (!more) break;
 			continue;
 		}
-		if (my >= 0 && !trace_step<F>(w.scene(rid), st)) {
+		const int cn = __popc(nmask), cl = __popc(lmask) * PSY_LEAF_WEIGHT, cp = __popc(pmask) * PSY_PATCH_WEIGHT;
+		const int run = (cp >= cl && cp >= cn) ? 3 : (cl >= cn) ? 2 : 1;
+		bool live = true;
+		if (kind == run) {
+			const DevScene& sc = w.scene(rid);
+			if (run == 1) {
+				const int r = walk_nodes<F>(sc, st, PSY_WALK_NODES);
+				live = r != WALK_DONE;
+				at_leaf = r == WALK_LEAF;
+			} else if (run == 2) {
+				at_leaf = false;
+				live = leaf_visit<F>(sc, st);
+			} else {
+				live = patch_step<F>(sc, st, PSY_PATCH_UNITS);
+			}
+		}
+		if (!live) {
 			err |= st.err;
 			if (OCCL) wb.occl[my] = st.rec.obj >= 0 ? 1 : 0;
 			else store_rec(wb, my, st.rec);

@@ -12,7 +12,7 @@
  * a level stack for nested assemblies (element id prefix, inherited shader,
  * merged motion transforms, as the reference's xform_stack /
  * surface_shader_stack / element_id, tracer/tracer.cpp:125-219), and the
- * path bits of the patch bisection (patch_intersect).
+ * path bits of the patch bisection (PatchWork, patch_run).
  */
 #ifndef PSY_TRACE_DEVICE_CUH
 #define PSY_TRACE_DEVICE_CUH
@@ -432,34 +432,83 @@ __device__ __forceinline__ bool patch_node_test(const Patch<NV> (&q)[TSC], float
 // needed.  The reference's stack index (its forced leaf at 63) is the number
 // of second halves on the path: the population count of the path bits.
 //
-// Returns true when a new closest hit was recorded (or, for occlusion rays,
-// when any leaf was hit).
+// The bisection can stop after any number of loop iterations and resume
+// later from PatchWork (the node at the top of the loop, whose box the ray
+// hits, with the path and the stored ancestors), so that a lane can leave a
+// long bisection to run with the other lanes of its warp.
 template <int NV, int TSC>
-__device__ bool patch_intersect(const float* verts, float time, const LocalRay& r, const RayWidth& rw, float* max_t,
-                                bool occl, float dice_rate, float min_upoly, PatchHit* hit) {
-	constexpr int CP = PSY_PATCH_CP_STEP;
-	constexpr int NCP = PSY_PATCH_CP_COUNT;
-	Patch<NV> cur[TSC];
+struct PatchCursor {
+	Patch<NV> cur[TSC];        // the node at the top of the loop
+	Bits128 path, dirs, pend;  // dirs bit: 1 = split along u
+	int depth;                 // splits from the root
+	float u0, u1, v0, v1;
+	float t_nalpha, max_dim, h0, h1;
+	bool found;
+};
+
+// Sub-patches stored on the current path (with their uv ranges).
+template <int NV, int TSC>
+struct PatchStore {
+	Patch<NV> cps[PSY_PATCH_CP_COUNT][TSC];
+	float cpuv[PSY_PATCH_CP_COUNT][4];
+};
+
+template <int NV, int TSC>
+struct PatchWork {
+	PatchCursor<NV, TSC> c;
+	PatchStore<NV, TSC> st;
+};
+
+// The root's test: sets up `pc` and returns true when the ray hits the
+// patch's box.
+template <int NV, int TSC>
+__device__ __forceinline__ bool patch_begin(PatchCursor<NV, TSC>& pc, const float* verts, float time,
+                                            const LocalRay& r, float max_t) {
 #pragma unroll
-	for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur[k]);
-	float t_nalpha = 0.0f;
+	for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &pc.cur[k]);
+	pc.t_nalpha = 0.0f;
 	if (TSC > 1) {
 		// bounds are lerped between the two samples; time == 1.0 would index
 		// past the last sample in the reference (undefined) and gives the
 		// first sample's bounds here
 		const float t_time = time * (float)(TSC - 1);
-		t_nalpha = t_time - (float)(int)t_time;
+		pc.t_nalpha = t_time - (float)(int)t_time;
 	}
-	float max_dim, h0, h1;
-	if (!patch_node_test<NV, TSC>(cur, t_nalpha, r, *max_t, &max_dim, &h0, &h1)) return false;
+	if (!patch_node_test<NV, TSC>(pc.cur, pc.t_nalpha, r, max_t, &pc.max_dim, &pc.h0, &pc.h1)) return false;
+	pc.path = Bits128{0, 0};
+	pc.dirs = Bits128{0, 0};
+	pc.pend = Bits128{0, 0};
+	pc.depth = 0;
+	pc.u0 = 0.0f;
+	pc.u1 = 1.0f;
+	pc.v0 = 0.0f;
+	pc.v1 = 1.0f;
+	pc.found = false;
+	return true;
+}
 
-	Patch<NV> cps[NCP][TSC];
-	float cpuv[NCP][4];
-	Bits128 path{0, 0}, dirs{0, 0}, pend{0, 0};  // dirs bit: 1 = split along u
-	int depth = 0;                                // splits from the root
-	float u0 = 0.0f, u1 = 1.0f, v0 = 0.0f, v1 = 1.0f;
-	bool found = false;
+// Runs up to `units` iterations of the bisection loop (a leaf test or a
+// split, with the resume that follows it).  Returns true when the
+// bisection has ended; pc.found then says whether a leaf was taken (the
+// closest one in *hit, with *max_t lowered to it; for occlusion rays the
+// first one).  Otherwise `pc` is the node to carry on from.
+template <int NV, int TSC>
+__device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<NV, TSC>& ps, const float* verts,
+                                          const LocalRay& r, const RayWidth& rw, float* max_t, bool occl,
+                                          float dice_rate, float min_upoly, PatchHit* hit, int units) {
+	constexpr int CP = PSY_PATCH_CP_STEP;
+	constexpr int NCP = PSY_PATCH_CP_COUNT;
+	Patch<NV>(&cur)[TSC] = pc.cur;
+	const float t_nalpha = pc.t_nalpha;
+	float &max_dim = pc.max_dim, &h0 = pc.h0, &h1 = pc.h1;
+	Bits128 &path = pc.path, &dirs = pc.dirs, &pend = pc.pend;
+	int& depth = pc.depth;
+	float &u0 = pc.u0, &u1 = pc.u1, &v0 = pc.v0, &v1 = pc.v1;
+	bool& found = pc.found;
+	auto& cps = ps.cps;
+	auto& cpuv = ps.cpuv;
 	while (true) {
+		if (units-- == 0) return false;
 		// `cur` is a node whose box the ray hits; max_dim, h0, h1 are its test
 		// A NaN width (from NaN ray differentials: a grazing hit makes the
 		// next ray's origin differentials 0/0 in transfer_ray_origin_
@@ -523,7 +572,7 @@ __device__ bool patch_intersect(const float* verts, float time, const LocalRay& 
 		// resume at the deepest pending first half whose box is still hit
 		while (true) {
 			const int j = pend.highest_below(depth);
-			if (j < 0) return found;
+			if (j < 0) return true;
 			pend.set(j, false);
 			path.set(j, false);
 			depth = j + 1;
@@ -566,6 +615,19 @@ __device__ bool patch_intersect(const float* verts, float time, const LocalRay& 
 	}
 }
 
+// The whole bisection of one patch in one call, its state in the caller's
+// frame.  Returns true when a leaf was taken.
+template <int NV, int TSC>
+__device__ bool patch_whole(const float* verts, float time, const LocalRay& r, const RayWidth& rw,
+                                            float* max_t, bool occl, float dice_rate, float min_upoly,
+                                            PatchHit* hit) {
+	PatchCursor<NV, TSC> pc;
+	PatchStore<NV, TSC> ps;
+	if (!patch_begin<NV, TSC>(pc, verts, time, r, *max_t)) return false;
+	patch_run<NV, TSC>(pc, ps, verts, r, rw, max_t, occl, dice_rate, min_upoly, hit, 0x7fffffff);
+	return pc.found;
+}
+
 // ---------------------------------------------------------------------
 // Whole-scene traversal
 // ---------------------------------------------------------------------
@@ -590,10 +652,26 @@ struct Level {
 	int inst_base;
 };
 
+// Patch kind of a bisection in progress: bilinear or bicubic, one or two
+// time samples.
+enum : int { PM_NONE = 0, PM_BILINEAR1, PM_BILINEAR2, PM_BICUBIC1, PM_BICUBIC2 };
+
+// Bytes of the bisection state for the patch kinds of feature set F.
+template <unsigned F>
+struct PatchBuf {
+	static constexpr int TS = (F & FEAT_PATCH_MOTION) ? 2 : 1;
+	static constexpr size_t b4 = (F & FEAT_BILINEAR) ? sizeof(PatchWork<4, TS>) : 0;
+	static constexpr size_t b16 = (F & FEAT_BICUBIC) ? sizeof(PatchWork<16, TS>) : 0;
+	static constexpr size_t m = b4 > b16 ? b4 : b16;
+	static constexpr size_t bytes = m > 16 ? m : 16;
+};
+
 // Traversal state of one ray.  trace_init sets it up; each trace_step
-// runs to the next object leaf and tests it, and returns false once the
-// ray is finished (rec and err then hold the result).  Kernels can refill
-// a lane with a new ray between steps.
+// runs to the next object leaf and tests it (a patch leaf whose box the
+// ray hits starts a bisection, which patch_step carries on), and
+// trace_step / patch_step return false once the ray is finished (rec and
+// err then hold the result).  Kernels can refill a lane with a new ray
+// between steps.
 template <unsigned F>
 struct TraceState {
 	WorldRayD wr;
@@ -606,9 +684,25 @@ struct TraceState {
 	LocalRay lvr[PSY_MAX_LEVELS];   // ray of each enclosing level, kept while a transformed child is traversed
 	int node_stack[PSY_NODE_STACK];
 	int nsp, L;
+	int leaf;                       // leaf popped by walk_nodes, for leaf_visit
 	LocalRay r;                     // the ray in the current level's space
 	RayWidth rw;                    // width parameters of r, valid when rw_ok
 	bool rw_ok;
+	// a patch leaf whose bisection is in progress (pmode != PM_NONE): its
+	// vertices, ray and widths, the hit record's fields, the bisection
+	int pmode;
+	int p_obj, p_kind, p_shader, p_gi;
+	uint64_t p_id;
+	const float* pverts;
+	LocalRay pr;
+	RayWidth prw;
+	PatchHit ph;
+	alignas(16) unsigned char pbuf[PatchBuf<F>::bytes];
+	template <int NV, int TSC>
+	__device__ __forceinline__ PatchWork<NV, TSC>& work() {
+		static_assert(sizeof(PatchWork<NV, TSC>) <= sizeof(pbuf), "patch work buffer");
+		return *reinterpret_cast<PatchWork<NV, TSC>*>(pbuf);
+	}
 };
 
 // F is a mask of FEAT_* scene features; code for absent features is not
@@ -633,172 +727,198 @@ __device__ __forceinline__ void trace_init(const DevScene& sc, TraceState<F>& s,
 	s.lvl_frame[0] = -1;
 	s.r = make_local(wr);
 	s.rw_ok = false;
+	s.pmode = PM_NONE;
 	const int root = sc.assemblies[0].root;
 	if (root != REF_EMPTY) s.node_stack[s.nsp++] = root;
 }
 
-// One step: (A) traverse to the next object leaf, (B) test it.  Running the
-// phases as separate loops lets the lanes of a warp run each phase together.
-// The closest hit does not depend on the order objects are tested in (a
-// sub-patch's box lies inside its parent's, so max_t pruning only drops
-// leaves that could not be closer), except for exact ties.
+// Records the hit on an object of the current level (Intersection fields
+// the traversal knows).  Returns false when the ray is finished: an
+// occlusion ray stops at its first hit.
 template <unsigned F>
-__device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s) {
+__device__ __forceinline__ bool trace_record(TraceState<F>& s, int obj, int kind, uint64_t id, int shader, int gi,
+                                             const PatchHit& ph) {
+	HitRec& rec = s.rec;
+	rec.obj = obj;
+	rec.kind = kind;
+	rec.id = id;
+	rec.shader = shader;
+	if (s.wr.occl) return false;
+	rec.t = ph.t;
+	rec.u = ph.u;
+	rec.v = ph.v;
+	rec.max_dim = ph.max_dim;
+	const int L = s.L;
+	rec.depth = L + 1;
+	for (int k = 1; k <= L; ++k) rec.path[k - 1] = s.lv[k].inst;
+	rec.path[L] = gi;
+	return true;
+}
+
+// An inner node: tests the child boxes (BBox4::intersect_ray,
+// basics/bbox.hpp:566-595) and pushes the hit children, nearest on top.
+// Returns false when the node stack overflows (the ray ends with an error).
+template <unsigned F>
+__device__ __forceinline__ bool node_visit(const DevScene& sc, TraceState<F>& s, int ref) {
+	const WorldRayD& wr = s.wr;
+	const DevNode* nd = sc.nodes + ref;
+	float b[24];
+	load_box4(reinterpret_cast<const float4*>(nd->b), b);
+	const int4 ch = __ldg(reinterpret_cast<const int4*>(nd->child));
+	const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->nchild));
+	const int nch = meta.x;
+	const int ts = meta.y;
+	if (ts > 1) {
+		// motion: lerp the boxes of the two time samples around the ray
+		// time (sample 0 is in the node, later ones in node_extra)
+		const SeqPos sp = seq_pos(wr.time, ts);
+		auto extra = [&](int k) {
+			return reinterpret_cast<const float4*>(sc.node_extra + (size_t)(meta.z + k - 1) * 24);
+		};
+		if (sp.single) {
+			if (sp.i0 != 0) load_box4(extra(sp.i0), b);
+		} else {
+			float e1[24];
+			load_box4(extra(sp.i0 + 1), e1);
+			if (sp.i0 != 0) load_box4(extra(sp.i0), b);
+			const float ia = one_minus(sp.nalpha);
+#pragma unroll
+			for (int i = 0; i < 24; ++i) b[i] = (b[i] * ia) + (e1[i] * sp.nalpha);
+		}
+	}
+	// slab tests of the four children; every array index below is a
+	// compile-time constant so the node stays in registers
+	const bool ds0 = s.r.dinv.x < 0.0f, ds1 = s.r.dinv.y < 0.0f, ds2 = s.r.dinv.z < 0.0f;
+	const int chv[4] = {ch.x, ch.y, ch.z, ch.w};
+	float tk[4];
+	int ck[4], sk[4];
+	int nhit = 0;
+#pragma unroll
+	for (int c = 0; c < 4; ++c) {
+		const float x0 = b[0 * 4 + c], x1 = b[1 * 4 + c];
+		const float y0 = b[2 * 4 + c], y1 = b[3 * 4 + c];
+		const float z0 = b[4 * 4 + c], z1 = b[5 * 4 + c];
+		const float xlo = ((ds0 ? x1 : x0) - s.r.o.x) * s.r.dinv.x;
+		const float xhi = ((ds0 ? x0 : x1) - s.r.o.x) * s.r.dinv.x;
+		const float ylo = ((ds1 ? y1 : y0) - s.r.o.y) * s.r.dinv.y;
+		const float yhi = ((ds1 ? y0 : y1) - s.r.o.y) * s.r.dinv.y;
+		const float zlo = ((ds2 ? z1 : z0) - s.r.o.z) * s.r.dinv.z;
+		const float zhi = ((ds2 ? z0 : z1) - s.r.o.z) * s.r.dinv.z;
+		const float mins = vmax(vmax(xlo, ylo), vmax(zlo, 0.0f));
+		const float maxs = vmax(vmin(vmin(xhi, yhi), zhi), -INFINITY) * BBOX_MAXT_ADJUST;
+		const bool h = c < nch && mins < s.max_t && mins <= maxs;
+		// a hit has mins < max_t <= inf, so inf marks the misses
+		tk[c] = h ? mins : INFINITY;
+		ck[c] = chv[c];
+		sk[c] = c;
+		nhit += h ? 1 : 0;
+	}
+	// nearest first, ties in child order (a stable sort by distance)
+	auto cswap = [&](int a, int bb) {
+		if (tk[bb] < tk[a] || (tk[bb] == tk[a] && sk[bb] < sk[a])) {
+			const float t = tk[a]; tk[a] = tk[bb]; tk[bb] = t;
+			const int c = ck[a]; ck[a] = ck[bb]; ck[bb] = c;
+			const int q = sk[a]; sk[a] = sk[bb]; sk[bb] = q;
+		}
+	};
+	if (s.nsp + nhit > PSY_NODE_STACK) {
+		s.err |= ERRF_STACK;
+		return false;
+	}
+	if (wr.occl) {
+		// an occlusion ray stops at any hit, so the order it meets the
+		// children in does not matter: push the hit ones unsorted
+#pragma unroll
+		for (int c = 3; c >= 0; --c)
+			if (tk[c] != INFINITY) s.node_stack[s.nsp++] = ck[c];
+		return true;
+	}
+	cswap(0, 1);
+	cswap(2, 3);
+	cswap(0, 2);
+	cswap(1, 3);
+	cswap(1, 2);
+	if (nhit > 3) s.node_stack[s.nsp++] = ck[3];
+	if (nhit > 2) s.node_stack[s.nsp++] = ck[2];
+	if (nhit > 1) s.node_stack[s.nsp++] = ck[1];
+	if (nhit > 0) s.node_stack[s.nsp++] = ck[0];
+	return true;
+}
+
+// Leaves the finished levels, restoring the ray of the enclosing level.
+template <unsigned F>
+__device__ __forceinline__ void leave_levels(TraceState<F>& s) {
 	constexpr bool NESTED = (F & FEAT_NESTED) != 0;
+	while (NESTED && s.L > 0 && s.nsp == s.lv[s.L].stack_base) {
+		const bool changed = s.lvl_frame[s.L] != s.lvl_frame[s.L - 1];
+		--s.L;
+		if (changed) {
+			s.r = s.lvr[s.L];
+			s.rw_ok = false;
+		}
+	}
+}
+
+// Enters the assembly of instance `inst` (global index gi, element id
+// `id`, inherited shader): merges its transforms into the level's frame,
+// moves the ray into its space and pushes its root.  Returns false when the
+// node stack overflows.
+template <unsigned F>
+__device__ __forceinline__ bool enter_assembly(const DevScene& sc, TraceState<F>& s, const DevInstance& inst, int gi,
+                                               uint64_t id, int shader) {
 	constexpr bool XFORM = (F & FEAT_XFORM) != 0;
 	const WorldRayD& wr = s.wr;
 	Frame none;
 	none.count = 0;
-	int gi = -1, local = 0, shader = -1;
-	uint64_t id = 0;
-	DevInstance inst;
-	while (true) {
-		// leave finished levels, restoring the ray of the enclosing level
-		while (NESTED && s.L > 0 && s.nsp == s.lv[s.L].stack_base) {
-			const bool changed = s.lvl_frame[s.L] != s.lvl_frame[s.L - 1];
-			--s.L;
-			if (changed) {
-				s.r = s.lvr[s.L];
-				s.rw_ok = false;
-			}
-		}
-		if (s.nsp == 0) return false;
-		const int ref = s.node_stack[--s.nsp];
-		if (ref >= 0) {
-			// inner node: test the child boxes (BBox4::intersect_ray, basics/bbox.hpp:566-595)
-			const DevNode* nd = sc.nodes + ref;
-			float b[24];
-			load_box4(reinterpret_cast<const float4*>(nd->b), b);
-			const int4 ch = __ldg(reinterpret_cast<const int4*>(nd->child));
-			const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->nchild));
-			const int nch = meta.x;
-			const int ts = meta.y;
-			if (ts > 1) {
-				// motion: lerp the boxes of the two time samples around the ray
-				// time (sample 0 is in the node, later ones in node_extra)
-				const SeqPos sp = seq_pos(wr.time, ts);
-				auto extra = [&](int k) {
-					return reinterpret_cast<const float4*>(sc.node_extra + (size_t)(meta.z + k - 1) * 24);
-				};
-				if (sp.single) {
-					if (sp.i0 != 0) load_box4(extra(sp.i0), b);
-				} else {
-					float e1[24];
-					load_box4(extra(sp.i0 + 1), e1);
-					if (sp.i0 != 0) load_box4(extra(sp.i0), b);
-					const float ia = one_minus(sp.nalpha);
-#pragma unroll
-					for (int i = 0; i < 24; ++i) b[i] = (b[i] * ia) + (e1[i] * sp.nalpha);
-				}
-			}
-			// slab tests of the four children; every array index below is a
-			// compile-time constant so the node stays in registers
-			const bool ds0 = s.r.dinv.x < 0.0f, ds1 = s.r.dinv.y < 0.0f, ds2 = s.r.dinv.z < 0.0f;
-			const int chv[4] = {ch.x, ch.y, ch.z, ch.w};
-			float tk[4];
-			int ck[4], sk[4];
-			int nhit = 0;
-#pragma unroll
-			for (int c = 0; c < 4; ++c) {
-				const float x0 = b[0 * 4 + c], x1 = b[1 * 4 + c];
-				const float y0 = b[2 * 4 + c], y1 = b[3 * 4 + c];
-				const float z0 = b[4 * 4 + c], z1 = b[5 * 4 + c];
-				const float xlo = ((ds0 ? x1 : x0) - s.r.o.x) * s.r.dinv.x;
-				const float xhi = ((ds0 ? x0 : x1) - s.r.o.x) * s.r.dinv.x;
-				const float ylo = ((ds1 ? y1 : y0) - s.r.o.y) * s.r.dinv.y;
-				const float yhi = ((ds1 ? y0 : y1) - s.r.o.y) * s.r.dinv.y;
-				const float zlo = ((ds2 ? z1 : z0) - s.r.o.z) * s.r.dinv.z;
-				const float zhi = ((ds2 ? z0 : z1) - s.r.o.z) * s.r.dinv.z;
-				const float mins = vmax(vmax(xlo, ylo), vmax(zlo, 0.0f));
-				const float maxs = vmax(vmin(vmin(xhi, yhi), zhi), -INFINITY) * BBOX_MAXT_ADJUST;
-				const bool h = c < nch && mins < s.max_t && mins <= maxs;
-				// a hit has mins < max_t <= inf, so inf marks the misses
-				tk[c] = h ? mins : INFINITY;
-				ck[c] = chv[c];
-				sk[c] = c;
-				nhit += h ? 1 : 0;
-			}
-			// nearest first, ties in child order (a stable sort by distance)
-			auto cswap = [&](int a, int bb) {
-				if (tk[bb] < tk[a] || (tk[bb] == tk[a] && sk[bb] < sk[a])) {
-					const float t = tk[a]; tk[a] = tk[bb]; tk[bb] = t;
-					const int c = ck[a]; ck[a] = ck[bb]; ck[bb] = c;
-					const int q = sk[a]; sk[a] = sk[bb]; sk[bb] = q;
-				}
-			};
-			if (s.nsp + nhit > PSY_NODE_STACK) {
-				s.err |= ERRF_STACK;
-				return false;
-			}
-			if (wr.occl) {
-				// an occlusion ray stops at any hit, so the order it meets the
-				// children in does not matter: push the hit ones unsorted
-#pragma unroll
-				for (int c = 3; c >= 0; --c)
-					if (tk[c] != INFINITY) s.node_stack[s.nsp++] = ck[c];
-				continue;
-			}
-			cswap(0, 1);
-			cswap(2, 3);
-			cswap(0, 2);
-			cswap(1, 3);
-			cswap(1, 2);
-			if (nhit > 3) s.node_stack[s.nsp++] = ck[3];
-			if (nhit > 2) s.node_stack[s.nsp++] = ck[2];
-			if (nhit > 1) s.node_stack[s.nsp++] = ck[1];
-			if (nhit > 0) s.node_stack[s.nsp++] = ck[0];
-			continue;
-		}
-
-
-		// leaf: one instance of the current level's assembly
-		local = leaf_instance(ref);
-		gi = s.lv[s.L].inst_base + local;
-		inst = sc.instances[gi];
-		id = id_push(s.lv[s.L].id, (uint64_t)local, s.lv[s.L].id_bits);
-		shader = inst.shader >= 0 ? inst.shader : s.lv[s.L].shader;
-
-		if (NESTED && inst.kind == INST_ASSEMBLY) {
-			const int L = s.L;
-			const Frame& parent = s.lvl_frame[L] >= 0 ? s.frames[s.lvl_frame[L]] : none;
-			if (L + 1 >= PSY_MAX_LEVELS) {
-				s.err |= ERRF_LEVELS;
-				continue;
-			}
-			const DevAssembly as = sc.assemblies[inst.data];
-			if (as.root == REF_EMPTY) continue;
-			if (XFORM && inst.xform_count > 0) {
-				if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &s.frames[L + 1])) {
-					s.err |= ERRF_MOTION;
-					continue;
-				}
-				s.lvl_frame[L + 1] = L + 1;
-				s.lvr[L] = s.r;
-				s.r = make_local_x(wr, frame_at_index_lerp(s.frames[L + 1], wr.time));
-				s.rw_ok = false;
-			} else {
-				s.lvl_frame[L + 1] = s.lvl_frame[L];
-			}
-			s.L = L + 1;
-			Level& nl = s.lv[L + 1];
-			nl.asmb = inst.data;
-			nl.stack_base = s.nsp;
-			nl.shader = shader;
-			nl.inst = gi;
-			nl.id = id;
-			nl.id_bits = as.id_bits;
-			nl.inst_base = as.inst_base;
-			if (s.nsp + 1 > PSY_NODE_STACK) {
-				s.err |= ERRF_STACK;
-				return false;
-			}
-			s.node_stack[s.nsp++] = as.root;
-			continue;
-		}
-		break;  // an object instance
+	const int L = s.L;
+	const Frame& parent = s.lvl_frame[L] >= 0 ? s.frames[s.lvl_frame[L]] : none;
+	if (L + 1 >= PSY_MAX_LEVELS) {
+		s.err |= ERRF_LEVELS;
+		return true;
 	}
+	const DevAssembly as = sc.assemblies[inst.data];
+	if (as.root == REF_EMPTY) return true;
+	if (XFORM && inst.xform_count > 0) {
+		if (!frame_merge(parent, sc.xforms + (size_t)inst.xform * 16, inst.xform_count, &s.frames[L + 1])) {
+			s.err |= ERRF_MOTION;
+			return true;
+		}
+		s.lvl_frame[L + 1] = L + 1;
+		s.lvr[L] = s.r;
+		s.r = make_local_x(wr, frame_at_index_lerp(s.frames[L + 1], wr.time));
+		s.rw_ok = false;
+	} else {
+		s.lvl_frame[L + 1] = s.lvl_frame[L];
+	}
+	s.L = L + 1;
+	Level& nl = s.lv[L + 1];
+	nl.asmb = inst.data;
+	nl.stack_base = s.nsp;
+	nl.shader = shader;
+	nl.inst = gi;
+	nl.id = id;
+	nl.id_bits = as.id_bits;
+	nl.inst_base = as.inst_base;
+	if (s.nsp + 1 > PSY_NODE_STACK) {
+		s.err |= ERRF_STACK;
+		return false;
+	}
+	s.node_stack[s.nsp++] = as.root;
+	return true;
+}
 
-	// (B) the object instance's test
+// The test of object instance `inst` of the current level (global index
+// gi, element id `id`, bound shader).  With RESUME a patch whose box the
+// ray hits only starts its bisection (patch_step carries it on); without,
+// the bisection runs here.  Returns false when the ray is finished (an
+// occlusion ray's hit).
+template <unsigned F, bool RESUME>
+__device__ __forceinline__ bool object_test(const DevScene& sc, TraceState<F>& s, const DevInstance& inst, int gi,
+                                            uint64_t id, int shader) {
+	constexpr bool XFORM = (F & FEAT_XFORM) != 0;
+	const WorldRayD& wr = s.wr;
+	Frame none;
+	none.count = 0;
 	const int L = s.L;
 	LocalRay lr = s.r;
 	M44 om;  // the object's own transform at the ray time
@@ -828,10 +948,44 @@ __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s)
 		}
 		return s.rw;
 	};
+	// a patch with RESUME: test the root box here, bisect in patch_step
+	auto begin_patch = [&](const float* v) {
+		int pm = PM_NONE;
+		if constexpr ((F & FEAT_BILINEAR) != 0) {
+			if (ob.kind == OBJ_BILINEAR) {
+				if constexpr ((F & FEAT_PATCH_MOTION) != 0) {
+					if (ob.n0 != 1)
+						pm = patch_begin<4, 2>(s.template work<4, 2>().c, v, wr.time, lr, s.max_t) ? PM_BILINEAR2 : -1;
+				}
+				if (pm == PM_NONE) pm = patch_begin<4, 1>(s.template work<4, 1>().c, v, wr.time, lr, s.max_t) ? PM_BILINEAR1 : -1;
+			}
+		}
+		if constexpr ((F & FEAT_BICUBIC) != 0) {
+			if (ob.kind == OBJ_BICUBIC) {
+				if constexpr ((F & FEAT_PATCH_MOTION) != 0) {
+					if (ob.n0 != 1)
+						pm = patch_begin<16, 2>(s.template work<16, 2>().c, v, wr.time, lr, s.max_t) ? PM_BICUBIC2 : -1;
+				}
+				if (pm == PM_NONE) pm = patch_begin<16, 1>(s.template work<16, 1>().c, v, wr.time, lr, s.max_t) ? PM_BICUBIC1 : -1;
+			}
+		}
+		if (pm > PM_NONE) {
+			s.pmode = pm;
+			s.pverts = v;
+			s.pr = lr;
+			s.prw = width();
+			s.p_obj = inst.data;
+			s.p_kind = ob.kind;
+			s.p_id = id;
+			s.p_shader = shader;
+			s.p_gi = gi;
+		}
+	};
 	bool hit = false;
 	PatchHit ph;
 	ph.u = ph.v = ph.max_dim = 0.0f;
 	float max_t = s.max_t;
+	const float* v = sc.fpool + ob.data;
 	if (ob.kind == OBJ_SPHERE || ob.kind == OBJ_SPHERE_LIGHT) {
 		V3 cent;
 		float radi;
@@ -847,37 +1001,126 @@ __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s)
 			ph.t = t;
 			if (!wr.occl) max_t = t;
 		}
-	} else if ((F & FEAT_BILINEAR) && ob.kind == OBJ_BILINEAR) {
-		const float* v = sc.fpool + ob.data;
-		const RayWidth w = width();
-		if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-			hit = patch_intersect<4, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
-		else
-			hit = patch_intersect<4, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
-	} else if ((F & FEAT_BICUBIC) && ob.kind == OBJ_BICUBIC) {
-		const float* v = sc.fpool + ob.data;
-		const RayWidth w = width();
-		if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-			hit = patch_intersect<16, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
-		else
-			hit = patch_intersect<16, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+	} else if constexpr (!RESUME) {
+		// the bisection runs here, to its end
+		if ((F & FEAT_BILINEAR) && ob.kind == OBJ_BILINEAR) {
+			const RayWidth w = width();
+			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
+				hit = patch_whole<4, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+			else
+				hit = patch_whole<4, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+		} else if ((F & FEAT_BICUBIC) && ob.kind == OBJ_BICUBIC) {
+			const RayWidth w = width();
+			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
+				hit = patch_whole<16, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+			else
+				hit = patch_whole<16, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+		}
+	} else {
+		begin_patch(v);
 	}
 	s.max_t = max_t;
-	if (hit) {
-		HitRec& rec = s.rec;
-		rec.obj = inst.data;
-		rec.kind = ob.kind;
-		rec.id = id;
-		rec.shader = shader;
-		if (wr.occl) return false;
-		rec.t = ph.t;
-		rec.u = ph.u;
-		rec.v = ph.v;
-		rec.max_dim = ph.max_dim;
-		rec.depth = L + 1;
-		for (int k = 1; k <= L; ++k) rec.path[k - 1] = s.lv[k].inst;
-		rec.path[L] = gi;
+	if (hit) return trace_record<F>(s, inst.data, ob.kind, id, shader, gi, ph);
+	return true;
+}
+
+// One step: traverse to the next object leaf and test it.  The closest hit
+// does not depend on the order objects are tested in (a sub-patch's box
+// lies inside its parent's, so max_t pruning only drops leaves that could
+// not be closer), except for exact ties.  Returns false when the ray is
+// finished.
+template <unsigned F, bool RESUME>
+__device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s) {
+	constexpr bool NESTED = (F & FEAT_NESTED) != 0;
+	while (true) {
+		leave_levels<F>(s);
+		if (s.nsp == 0) return false;
+		const int ref = s.node_stack[--s.nsp];
+		if (ref >= 0) {
+			if (!node_visit<F>(sc, s, ref)) return false;
+			continue;
+		}
+		// leaf: one instance of the current level's assembly
+		const int local = leaf_instance(ref);
+		const int gi = s.lv[s.L].inst_base + local;
+		const DevInstance inst = sc.instances[gi];
+		const uint64_t id = id_push(s.lv[s.L].id, (uint64_t)local, s.lv[s.L].id_bits);
+		const int shader = inst.shader >= 0 ? inst.shader : s.lv[s.L].shader;
+		if (NESTED && inst.kind == INST_ASSEMBLY) {
+			if (!enter_assembly<F>(sc, s, inst, gi, id, shader)) return false;
+			continue;
+		}
+		return object_test<F, RESUME>(sc, s, inst, gi, id, shader);
 	}
+}
+
+// The walk cut into pieces for kernels that group their lanes by the work
+// they do next: up to `nodes` inner-node visits, stopping at a leaf, which
+// is popped into s.leaf for leaf_visit.  Returns WALK_DONE when the ray is
+// finished, WALK_LEAF at a leaf, WALK_MORE when the visits ran out.
+enum : int { WALK_DONE = 0, WALK_LEAF = 1, WALK_MORE = 2 };
+
+template <unsigned F>
+__device__ __forceinline__ int walk_nodes(const DevScene& sc, TraceState<F>& s, int nodes) {
+	while (true) {
+		leave_levels<F>(s);
+		if (s.nsp == 0) return WALK_DONE;
+		const int ref = s.node_stack[s.nsp - 1];
+		if (ref < 0) {
+			--s.nsp;
+			s.leaf = ref;
+			return WALK_LEAF;
+		}
+		if (nodes-- == 0) return WALK_MORE;
+		--s.nsp;
+		if (!node_visit<F>(sc, s, ref)) return WALK_DONE;
+	}
+}
+
+// The leaf popped by walk_nodes: an assembly instance is entered, an object
+// instance tested (a patch starts its bisection).  Returns false when the
+// ray is finished.
+template <unsigned F>
+__device__ __forceinline__ bool leaf_visit(const DevScene& sc, TraceState<F>& s) {
+	constexpr bool NESTED = (F & FEAT_NESTED) != 0;
+	const int local = leaf_instance(s.leaf);
+	const int gi = s.lv[s.L].inst_base + local;
+	const DevInstance inst = sc.instances[gi];
+	const uint64_t id = id_push(s.lv[s.L].id, (uint64_t)local, s.lv[s.L].id_bits);
+	const int shader = inst.shader >= 0 ? inst.shader : s.lv[s.L].shader;
+	if (NESTED && inst.kind == INST_ASSEMBLY) return enter_assembly<F>(sc, s, inst, gi, id, shader);
+	return object_test<F, true>(sc, s, inst, gi, id, shader);
+}
+
+// Carries the bisection in progress on for up to `units` iterations of its
+// loop.  Returns false when the ray is finished (an occlusion ray's hit).
+template <unsigned F>
+__device__ __forceinline__ bool patch_step(const DevScene& sc, TraceState<F>& s, int units) {
+	constexpr int TS = PatchBuf<F>::TS;
+	bool done = false, found = false;
+	float max_t = s.max_t;
+	const bool occl = s.wr.occl;
+	const float dr = sc.dice_rate, mu = sc.min_upoly_size;
+	// the cursor runs as a local copy (registers) and goes back to the
+	// state only when the bisection stops short of its end
+	auto run = [&](auto& pw) {
+		auto pc = pw.c;
+		done = patch_run(pc, pw.st, s.pverts, s.pr, s.prw, &max_t, occl, dr, mu, &s.ph, units);
+		if (!done) pw.c = pc;
+		found = pc.found;
+	};
+	if constexpr ((F & FEAT_BILINEAR) != 0) {
+		if (s.pmode == PM_BILINEAR1) run(s.template work<4, 1>());
+		else if (TS == 2 && s.pmode == PM_BILINEAR2) run(s.template work<4, TS>());
+	}
+	if constexpr ((F & FEAT_BICUBIC) != 0) {
+		if (s.pmode == PM_BICUBIC1) run(s.template work<16, 1>());
+		else if (TS == 2 && s.pmode == PM_BICUBIC2) run(s.template work<16, TS>());
+	}
+	s.max_t = max_t;
+	if (!done) return true;
+	s.pmode = PM_NONE;
+	if (found) return trace_record<F>(s, s.p_obj, s.p_kind, s.p_id, s.p_shader, s.p_gi, s.ph);
 	return true;
 }
 
@@ -886,7 +1129,7 @@ template <unsigned F>
 __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
 	TraceState<F> s;
 	trace_init<F>(sc, s, wr);
-	while (trace_step<F>(sc, s)) {
+	while (trace_step<F, false>(sc, s)) {
 	}
 	*rec = s.rec;
 	return s.err;
