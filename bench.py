@@ -41,7 +41,7 @@ BYTES_PER_OCCLUSION_RAY = 64
 # DRAM bytes per traced ray of the traversal kernel, from the ncu capture in
 # profiles/trace_wave_kernel_many_light_640x360x4.md (dram read + write of the
 # camera launch / its 921,600 rays)
-TRAFFIC_BYTES_PER_RAY = 1868.0
+TRAFFIC_BYTES_PER_RAY = 4972.6
 BYTES_PER_PATH_EXTRA = 20   # sampler seed 4 + pixel 4 + XYZ 12
 RENDER_RES = (1280, 720)
 RENDER_SPP = 64
@@ -249,8 +249,12 @@ def render_workload():
 
 
 RENDER_METRIC = "paths/s at 720p (1280x720, 64 spp, 6 segments, many-light scene)"
-RENDER_WORKLOAD = ("render: 1280x720 x 64 spp, 6 segments; 2,000 bicubic patches, 500 sphere groups through 3 "
-                   "assembly levels with transform motion, 10,000 sphere lights (light tree + MIS), DoF, camera motion")
+
+
+def render_workload_name():
+    return ("render: %dx%d x %d spp, %d segments; 2,000 bicubic patches, 500 sphere groups through 3 assembly levels "
+            "with transform motion, 10,000 sphere lights (light tree + MIS), DoF, camera motion"
+            % (RENDER_RES[0], RENDER_RES[1], RENDER_SPP, RENDER_PATH_LENGTH))
 
 
 def run_render_ours(args, rank, local, pg, world):
@@ -327,7 +331,7 @@ def run_render_ours(args, rank, local, pg, world):
         "metric": RENDER_METRIC, "value": round(value, 1), "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded many-light scene)",
-        "config": {"workload": RENDER_WORKLOAD, "paths_per_step": paths, "path_length": RENDER_PATH_LENGTH,
+        "config": {"workload": render_workload_name(), "paths_per_step": paths, "path_length": RENDER_PATH_LENGTH,
                    "stream_paths": args.stream_paths or "auto (2^21)",
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "per-path state (~200 B x 2M paths in flight) larger than L2"},
@@ -417,7 +421,7 @@ def run_render_reference(args, spp: int = 2):
     return {"metric": RENDER_METRIC, "impl": "reference", "value": round(value, 1), "unit": "paths/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded many-light scene)",
-            "config": {"workload": RENDER_WORKLOAD, "sample_paths_per_step": paths},
+            "config": {"workload": render_workload_name(), "sample_paths_per_step": paths},
             "mrays_per_s": round(rays / tot / 1e6, 3),
             "cpu_baseline": {"value": round(value, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
                              "sample": "the 1280x720 frame at %d spp per step (%d paths), PathTraceIntegrator::"
