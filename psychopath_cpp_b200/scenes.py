@@ -19,6 +19,8 @@ generated from a seed:
                        with 2-sample transform motion, 10,000 sphere lights
                        (r 0.05, power log-uniform [1,1000]), depth of field
                        (aperture 0.05) and camera motion.
+* ``motion_patch_scene`` bilinear and bicubic patches with two time samples
+                       (patch motion), for parity tests.
 * ``batch_scenes``     48 renders of random size/spp/light count.
 """
 from __future__ import annotations
@@ -221,6 +223,49 @@ def _bezier_surface_patch(x0, y0, size, rng, jitter) -> np.ndarray:
             pts.append([x, y, z])
     pts = np.array(pts) + rng.normal(0.0, jitter, size=(16, 3))
     return pts.astype(np.float32)
+
+
+def motion_patch_scene(seed: int = 1, res=(96, 72), spp: int = 8, n: int = 6) -> Scene:
+    """Patches that move and deform while the shutter is open: an n x n grid
+    of alternating bilinear and bicubic patches, each with two time samples
+    (the second sample shifted by up to 0.3 and its control points jittered
+    by N(0, 0.05)), over a static ground patch, with a few Lambert spheres
+    and one sphere light; pinhole camera without motion."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(name="motion_patch_%d" % seed, res_x=res[0], res_y=res[1], spp=spp, seed=1)
+    sc.camera = Camera(transforms=[look_at((0.0, -9.0, 6.0), (0.0, 0.0, 0.3))], fovs=[50.0])
+    root = sc.root
+    root.add_shader("ground", SurfaceShader("Lambert", [0.5, 0.5, 0.5]))
+    root.add_object("ground", BilinearPatch([[-8, -8, 0], [8, -8, 0], [-8, 8, 0], [8, 8, 0]]))
+    root.add_instance("ground", shader="ground")
+    size = 6.0 / n
+    for j in range(n):
+        for i in range(n):
+            k = j * n + i
+            x0, y0 = -3.0 + i * size, -3.0 + j * size
+            shift = np.array([rng.uniform(-0.3, 0.3), rng.uniform(-0.3, 0.3), rng.uniform(0.0, 0.3)])
+            if k % 2 == 0:
+                z = rng.uniform(0.3, 0.9, 4)
+                v0 = np.array([[x0, y0, z[0]], [x0 + size, y0, z[1]], [x0, y0 + size, z[2]],
+                               [x0 + size, y0 + size, z[3]]])
+                v1 = v0 + shift + rng.normal(0.0, 0.05, (4, 3))
+                obj = BilinearPatch(np.stack([v0, v1]))
+            else:
+                v0 = _bezier_surface_patch(x0, y0, size, rng, 0.1) + np.array([0.0, 0.0, 0.6])
+                v1 = v0 + shift + rng.normal(0.0, 0.05, (16, 3))
+                obj = BicubicPatch(np.stack([v0, v1]))
+            alb = rng.uniform(0.3, 0.8)
+            root.add_shader("m%d" % k, SurfaceShader("Lambert", [alb, 0.5, 1.0 - alb]))
+            root.add_object("p%d" % k, obj)
+            root.add_instance("p%d" % k, shader="m%d" % k)
+    for i in range(4):
+        c = [rng.uniform(-3, 3), rng.uniform(-3, 3), rng.uniform(1.2, 1.8)]
+        root.add_shader("s%d" % i, SurfaceShader("Lambert", [0.7] * 3))
+        root.add_object("sphere%d" % i, Sphere(c, rng.uniform(0.2, 0.4)))
+        root.add_instance("sphere%d" % i, shader="s%d" % i)
+    root.add_object("light", SphereLight([[1.0, -1.0, 5.0]], [0.6], [[80.0] * 3]))
+    root.add_instance("light")
+    return sc
 
 
 def many_light_scene(seed: int = 3, res=(1280, 720), spp: int = 64, n_patches: int = 2000,

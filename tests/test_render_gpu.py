@@ -104,6 +104,18 @@ def test_many_light_instanced_render(ctx, ref_available):
     assert err <= 1e-2, err
 
 
+def test_motion_patch_render(ctx, ref_available):
+    """Patch motion in the wave kernels, where a bisection stops and resumes
+    between warp iterations (both patch kinds with two time samples)."""
+    sc = scenes.motion_patch_scene(1, res=(96, 72), spp=8)
+    (rx, rc, rrays), (mx, mc, mrays) = _render_both(ctx, sc, 8, 4)
+    assert (rc == mc).all()
+    err, npx = rel_rmse(mx, rx)
+    assert npx > 3000
+    assert err <= IMAGE_REL_RMSE, err
+    assert abs(int(rrays) - int(mrays)) <= 0.001 * rrays, (rrays, mrays)
+
+
 def test_render_rejects_bad_arguments(ctx):
     sc = scenes.plain_scene(1, res=(8, 8), spp=1)
     ctx.upload(sc)

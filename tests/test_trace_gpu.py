@@ -87,6 +87,19 @@ def test_instanced_motion_bicubic_scene(ctx, ref_available):
     parity.assert_parity(rep)
 
 
+def test_motion_patches(ctx, ref_available):
+    """Bilinear and bicubic patches with two time samples: the bisection
+    lerps each sub-patch's bounds to the ray time."""
+    sc = scenes.motion_patch_scene(2)
+    cam = _camera_rays(sc, 12000, 5)
+    rnd = parity.random_rays(12000, (-4, -4, 0.05), (4, 4, 2), seed=9, occl_frac=0.4)
+    rays = parity.concat_rays(cam, rnd)
+    ref, mine = _trace_both(ctx, sc, rays, fields=("hit", "id", "t", "uv", "closure"))
+    rep = parity.compare_trace(ref, mine, rays["type"], uv_mask=mine["closure"] != 2)
+    parity.assert_parity(rep)
+    assert rep["closest_hits"] > 10000
+
+
 GEOM = ("hit", "id", "t", "uv", "p", "n", "dpdu", "dpdv", "backfacing", "light_pdf", "offset", "space",
         "closure", "closure_color")
 
