@@ -433,9 +433,11 @@ __device__ __forceinline__ bool patch_node_test(const Patch<NV> (&q)[TSC], float
 // of second halves on the path: the population count of the path bits.
 //
 // The bisection can stop after any number of loop iterations and resume
-// later from PatchWork (the node at the top of the loop, whose box the ray
-// hits, with the path and the stored ancestors), so that a lane can leave a
-// long bisection to run with the other lanes of its warp.
+// later from its cursor (the node at the top of the loop, whose box the ray
+// hits, with its path bits and uv range) and its stored ancestors, so that
+// a lane can leave a long bisection to run with the other lanes of its
+// warp.  patch_run works on a cursor the caller holds as a local (kept in
+// registers) and copies back only when it stops short of the end.
 template <int NV, int TSC>
 struct PatchCursor {
 	Patch<NV> cur[TSC];        // the node at the top of the loop
@@ -453,6 +455,7 @@ struct PatchStore {
 	float cpuv[PSY_PATCH_CP_COUNT][4];
 };
 
+// A suspended bisection in a lane's traversal state.
 template <int NV, int TSC>
 struct PatchWork {
 	PatchCursor<NV, TSC> c;
@@ -666,12 +669,12 @@ struct PatchBuf {
 	static constexpr size_t bytes = m > 16 ? m : 16;
 };
 
-// Traversal state of one ray.  trace_init sets it up; each trace_step
-// runs to the next object leaf and tests it (a patch leaf whose box the
-// ray hits starts a bisection, which patch_step carries on), and
-// trace_step / patch_step return false once the ray is finished (rec and
-// err then hold the result).  Kernels can refill a lane with a new ray
-// between steps.
+// Traversal state of one ray.  trace_init sets it up.  A lane that runs
+// its ray alone calls trace_step (to the next object leaf and its test)
+// until it returns false; the wave kernels advance it in pieces instead
+// (walk_nodes, leaf_visit, patch_step, each returning false once the ray
+// is finished).  rec and err then hold the result.  Kernels can refill a
+// lane with a new ray between pieces.
 template <unsigned F>
 struct TraceState {
 	WorldRayD wr;
@@ -1024,12 +1027,13 @@ __device__ __forceinline__ bool object_test(const DevScene& sc, TraceState<F>& s
 	return true;
 }
 
-// One step: traverse to the next object leaf and test it.  The closest hit
+// One step of a lane that runs its ray alone: traverse to the next object
+// leaf and test it, a patch's whole bisection included.  The closest hit
 // does not depend on the order objects are tested in (a sub-patch's box
 // lies inside its parent's, so max_t pruning only drops leaves that could
 // not be closer), except for exact ties.  Returns false when the ray is
 // finished.
-template <unsigned F, bool RESUME>
+template <unsigned F>
 __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s) {
 	constexpr bool NESTED = (F & FEAT_NESTED) != 0;
 	while (true) {
@@ -1050,7 +1054,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s)
 			if (!enter_assembly<F>(sc, s, inst, gi, id, shader)) return false;
 			continue;
 		}
-		return object_test<F, RESUME>(sc, s, inst, gi, id, shader);
+		return object_test<F, false>(sc, s, inst, gi, id, shader);
 	}
 }
 
@@ -1129,7 +1133,7 @@ template <unsigned F>
 __device__ unsigned trace_ray(const DevScene& sc, const WorldRayD& wr, HitRec* rec) {
 	TraceState<F> s;
 	trace_init<F>(sc, s, wr);
-	while (trace_step<F, false>(sc, s)) {
+	while (trace_step<F>(sc, s)) {
 	}
 	*rec = s.rec;
 	return s.err;
