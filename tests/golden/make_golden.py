@@ -30,6 +30,7 @@ SCENES = {
     "heightfield": ("heightfield_scene", {"n": 16, "seed": 2}),
     "instanced": ("many_light_scene", {"seed": 5, "res": [64, 36], "spp": 1, "n_patches": 40, "n_groups": 20,
                                        "n_lights": 100}),
+    "motion": ("motion_patch_scene", {"seed": 2, "n": 4}),
 }
 
 
@@ -46,6 +47,8 @@ def rays_for(name):
         return parity.random_rays(2048, (-6, -6, 0.01), (6, 6, 3), seed=31, occl_frac=0.3)
     if name == "heightfield":
         return scenes.heightfield_rays(2048, n=16, seed=32)
+    if name == "motion":
+        return parity.random_rays(2048, (-4, -4, 0.05), (4, 4, 2), seed=34, occl_frac=0.3)
     return parity.random_rays(2048, (-8, -6, -0.5), (8, 6, 5), seed=33, occl_frac=0.3)
 
 

@@ -51,7 +51,7 @@ def _compare_bvh4(ref, mine, transformed: bool):
         assert parity.ulp_diff(rb.astype(np.float32), mb.astype(np.float32)).max() == 0
 
 
-@pytest.mark.parametrize("name", ["plain", "heightfield", "instanced"])
+@pytest.mark.parametrize("name", ["plain", "heightfield", "instanced", "motion"])
 def test_bvh4_matches_reference_golden(name):
     g = np.load(os.path.join(GOLDEN, "accel_%s.npz" % name))
     sc = make_golden.make_scene(name)

@@ -48,7 +48,7 @@ def test_instance_id_packing():
     assert (v >> 17) & 0x1 == 1
 
 
-@pytest.mark.parametrize("name", ["plain", "heightfield", "instanced"])
+@pytest.mark.parametrize("name", ["plain", "heightfield", "instanced", "motion"])
 def test_port_trace_matches_reference_golden(name):
     g = np.load(os.path.join(GOLDEN, "trace_%s.npz" % name))
     rays = {k[4:]: g[k] for k in g.files if k.startswith("ray_")}

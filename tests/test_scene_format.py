@@ -19,13 +19,18 @@ def test_float_formatting_round_trips_through_float32():
 @pytest.mark.parametrize("make", [lambda: scenes.plain_scene(1),
                                   lambda: scenes.heightfield_scene(8),
                                   lambda: scenes.many_light_scene(2, res=(32, 18), spp=2, n_patches=12,
-                                                                  n_groups=10, n_lights=20)])
+                                                                  n_groups=10, n_lights=20),
+                                  lambda: scenes.motion_patch_scene(1, n=3)])
 def test_write_parse_round_trip(make):
     sc = make()
     txt = sc.to_psy()
     back = S.parse_psy(txt)
     assert back.to_psy() == txt
     assert back.res_x == sc.res_x and back.spp == sc.spp and back.seed == sc.seed
+    # per-object time samples survive (patch motion: two Vertices blocks)
+    for name, obj in sc.root.objects.items():
+        if hasattr(obj, "verts"):
+            assert back.root.objects[name].verts.shape == obj.verts.shape
 
 
 def test_parser_handles_comments_escapes_and_defaults():
