@@ -396,8 +396,8 @@ def render_cpu_baseline(spp: int = 4):
     paths = RENDER_RES[0] * RENDER_RES[1] * spp
     return {"value": round(paths / secs, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
             "mrays_per_s": round(rays / secs / 1e6, 3),
-            "sample": "the 1280x720 frame at %d spp (%d paths) instead of 64, PathTraceIntegrator::integrate on "
-                      "%d threads" % (spp, paths, threads)}
+            "sample": "the %dx%d frame at %d spp (%d paths) instead of %d, PathTraceIntegrator::integrate on "
+                      "%d threads" % (RENDER_RES[0], RENDER_RES[1], spp, paths, RENDER_SPP, threads)}
 
 
 def run_render_reference(args, spp: int = 2):
@@ -424,8 +424,9 @@ def run_render_reference(args, spp: int = 2):
             "config": {"workload": render_workload_name(), "sample_paths_per_step": paths},
             "mrays_per_s": round(rays / tot / 1e6, 3),
             "cpu_baseline": {"value": round(value, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
-                             "sample": "the 1280x720 frame at %d spp per step (%d paths), PathTraceIntegrator::"
-                                       "integrate on %d threads" % (spp, paths, threads)},
+                             "sample": "the %dx%d frame at %d spp per step (%d paths), PathTraceIntegrator::"
+                                       "integrate on %d threads" % (RENDER_RES[0], RENDER_RES[1], spp, paths,
+                                                                    threads)},
             "e2e": {"value": round(value, 1), "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -540,6 +541,116 @@ def run_batch_ours(args, rank, local, pg, world):
     }
 
 
+def _ref_batch_child(q, start, passes):
+    """Renders batch scenes start.. in order, each `passes` times at 1 spp,
+    and reports each scene's passes as soon as they are done."""
+    from oracle import psyref
+    from psychopath_cpp_b200 import scenes
+    threads = os.cpu_count() or 1
+    cfgs = scenes.batch_configs(48, seed=0)
+    for i in range(start, len(cfgs)):
+        c = cfgs[i]
+        ref = psyref.RefScene(scene=scenes.batch_scene(c["seed"], c["res"], 1, c["n_prims"], c["n_lights"]))
+        out = []
+        for _ in range(passes):
+            _, _, r, t = ref.render(threads=threads, spp=1, path_length=4, seed=c["seed"] + 1)
+            out.append((c["res"][0] * c["res"][1], r, t))
+        q.put((i, out))
+    q.put(None)
+
+
+def ref_batch_bounded(passes: int, scene_limit_s: float = 30.0):
+    """The reference's PathTraceIntegrator::integrate over the 48 batch
+    renders, each at 1 spp, `passes` times, in spawned child processes.  A
+    scene whose renders do not finish within scene_limit_s (a ray with NaN
+    differentials makes the reference's patch bisection run without end) is
+    left out: its child is stopped and a new one carries on with the next
+    scene.  Returns ([(paths, rays, seconds)] per pass, [left-out scenes])."""
+    import multiprocessing as mp
+    import queue as queue_mod
+    ctx = mp.get_context("spawn")
+    per_pass = [[0, 0, 0.0] for _ in range(passes)]
+    skipped = []
+    start = 0
+    while start < 48:
+        q = ctx.Queue()
+        p = ctx.Process(target=_ref_batch_child, args=(q, start, passes))
+        p.start()
+        while True:
+            try:
+                item = q.get(timeout=scene_limit_s)
+            except queue_mod.Empty:
+                p.kill()
+                p.join()
+                skipped.append(start)
+                start += 1
+                break
+            if item is None:
+                p.join()
+                start = 48
+                break
+            i, out = item
+            for k, (paths, rays, secs) in enumerate(out):
+                per_pass[k][0] += paths
+                per_pass[k][1] += rays
+                per_pass[k][2] += secs
+            start = i + 1
+    return [tuple(x) for x in per_pass], skipped
+
+
+def _batch_sample(threads, skipped):
+    s = "the 48 renders at 1 spp each, one after another, PathTraceIntegrator::integrate on %d threads" % threads
+    if skipped:
+        s += ("; left out: render(s) %s, whose reference render did not finish within 30 s (NaN ray differentials "
+              "stall its patch bisection)" % ", ".join(str(k) for k in skipped))
+    return s
+
+
+def batch_cpu_baseline():
+    from oracle import psyref
+    if not psyref.available():
+        return None
+    out, skipped = ref_batch_bounded(1)
+    paths, rays, secs = out[0]
+    if secs <= 0.0:
+        return None
+    threads = os.cpu_count() or 1
+    return {"value": round(paths / secs, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
+            "mrays_per_s": round(rays / secs / 1e6, 3), "sample": _batch_sample(threads, skipped)}
+
+
+def run_batch_reference(args):
+    """The reference has no batched renderer: its arm renders the 48 scenes
+    one after another with PathTraceIntegrator, each at 1 spp per step."""
+    from oracle import psyref
+    if not psyref.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libpsyref.so (the reference built from source) is missing"}
+    out, skipped = ref_batch_bounded(args.warmup + args.steps)
+    timed_passes = out[args.warmup:]
+    paths = sum(o[0] for o in timed_passes)
+    rays = sum(o[1] for o in timed_passes)
+    secs = sum(o[2] for o in timed_passes)
+    threads = os.cpu_count() or 1
+    if secs <= 0.0:
+        return {"impl": "reference", "unavailable": "none of the reference's batch renders finished"}
+    value = paths / secs
+    return {"metric": BATCH_METRIC, "impl": "reference", "value": round(value, 1), "unit": "paths/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs * 1e3 / args.steps, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (48 seeded scenes: spheres + bilinear patches)",
+            "config": {"workload": "batch: 48 renders, 64x64..1024x768, 10-50,000 primitives, 1-100 lights, "
+                                   "4 segments", "sample_paths_per_step": paths // args.steps},
+            "mrays_per_s": round(rays / secs / 1e6, 3),
+            "cpu_baseline": {"value": round(value, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
+                             "sample": _batch_sample(threads, skipped)},
+            "e2e": {"value": round(value, 1), "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_adjoint_reference(args):
+    return {"impl": "reference", "unavailable": "the reference has no differentiable render or adjoint (it shades "
+                                                "fixed RGB albedos and emission)"}
+
+
 ADJOINT_METRIC = "adjoint/forward time ratio (path-replay adjoint vs differentiable forward render)"
 
 
@@ -640,7 +751,8 @@ def main():
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         if rank == 0:
-            fn = run_render_reference if args.workload == "render" else run_trace_reference
+            fn = {"render": run_render_reference, "trace": run_trace_reference, "batch": run_batch_reference,
+                  "adjoint": run_adjoint_reference}[args.workload]
             print(json.dumps(fn(args)))
         if pg:
             pg.barrier()
@@ -655,8 +767,9 @@ def main():
     else:
         res = run_trace_ours(args, rank, local, pg, world)
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline and args.workload in ("render", "trace"):
-            res["cpu_baseline"] = render_cpu_baseline() if args.workload == "render" else trace_cpu_baseline()
+        if world == 1 and not args.no_cpu_baseline and args.workload in ("render", "trace", "batch"):
+            res["cpu_baseline"] = {"render": render_cpu_baseline, "trace": trace_cpu_baseline,
+                                   "batch": batch_cpu_baseline}[args.workload]()
         print(json.dumps(res))
     if pg:
         pg.barrier()
