@@ -67,3 +67,17 @@ def test_single_process_needs_no_group():
         for k, v in saved.items():
             if v is not None:
                 os.environ[k] = v
+
+
+def test_reference_arm_names_every_workload():
+    """Every workload has a reference arm; the adjoint one reports that the
+    reference has no differentiable render."""
+    sys.path.insert(0, ROOT)
+    import bench
+    import types
+    out = bench.run_adjoint_reference(types.SimpleNamespace(steps=1, warmup=3))
+    assert out["impl"] == "reference" and "unavailable" in out
+    for name in ("run_render_reference", "run_trace_reference", "run_batch_reference", "run_adjoint_reference"):
+        assert callable(getattr(bench, name))
+    s = bench._batch_sample(8, [14, 26])
+    assert "8 threads" in s and "14, 26" in s
