@@ -234,9 +234,13 @@ def trace_cpu_baseline(seconds_target: float = 10.0):
     for _ in range(3):
         secs.append(ref.trace(rays, threads=threads, chunk=65536, full=False)["seconds"])
     s = max(min(secs), 1e-9)
+    s1 = ref.trace(rays, threads=1, chunk=65536, full=False)["seconds"]
     return {"value": round(n / s / 1e6, 4), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "cpu_model": cpu_model(),
             "sample": "the whole 4,194,304-ray stream, Tracer::trace in 65,536-ray chunks on %d threads, "
-                      "best of 3" % threads}
+                      "best of 3" % threads,
+            "one_core": {"value": round(n / max(s1, 1e-9) / 1e6, 4), "unit": "Mrays/s", "cores": 1,
+                         "sample": "the whole stream once on 1 thread"}}
 
 
 # --------------------------------------------------------------------------
@@ -278,6 +282,9 @@ def run_render_ours(args, rank, local, pg, world):
     rays_per_render = int(integ.stats.rays)
     occl_per_render = int(integ.stats.occlusion_rays)
     launches_per_render = int(integ.stats.launches)
+    # every wave launches one closest-hit and one occlusion traversal per segment
+    trace_launches_per_render = int(integ.stats.waves) * 2 * RENDER_PATH_LENGTH
+    counters = ctx.trace_counters()
     paths = w * h * RENDER_SPP
     if pg:
         pg.barrier()
@@ -308,7 +315,10 @@ def run_render_ours(args, rank, local, pg, world):
     # closest-hit ray, 64 B per occlusion ray) over their own launch time
     closest = rays_per_render - occl_per_render
     trace_bytes = (closest * BYTES_PER_CLOSEST_RAY + occl_per_render * BYTES_PER_OCCLUSION_RAY) * args.steps
-    n_trace = max(1, int(trace_launches.value))
+    n_trace = int(trace_launches.value)
+    if n_trace != trace_launches_per_render * args.steps:
+        raise RuntimeError("timed %d traversal launches, expected %d x %d steps" %
+                           (n_trace, trace_launches_per_render, args.steps))
     achieved = trace_bytes / (trace_ms.value * 1e-3) / 1e9 if trace_ms.value > 0 else 0.0
     traffic = TRAFFIC_BYTES_PER_RAY * rays_per_render * args.steps / n_trace
     # end to end: the public call plus the device->host read of the film each step
@@ -348,18 +358,45 @@ def run_render_ours(args, rank, local, pg, world):
                 "h2d_bytes_per_step": 28, "d2h_bytes_per_step": w * h * 16},
         "gpu_launches": launches_per_render * args.steps,
         "clocks": clk.summary(),
+        "traversal_counters": per_ray_counters(counters),
     }
 
 
-def _ref_render_child(q, res, spp, path_length):
+def per_ray_counters(c: dict) -> dict:
+    """Traversal work per ray of one render (psy_profile_counters): node
+    visits, leaf visits and patch bisection iterations per ray, and the lanes
+    of 32 that ran work per traversal warp-loop iteration."""
+    out = {}
+    for kind in ("closest", "occlusion"):
+        k = c[kind]
+        n = max(1, k["rays"])
+        out[kind] = {"rays": k["rays"], "node_visits_per_ray": round(k["node_visits"] / n, 2),
+                     "leaf_visits_per_ray": round(k["leaf_visits"] / n, 2),
+                     "patch_iterations_per_ray": round(k["patch_iterations"] / n, 2),
+                     "lanes_per_warp_step": round(k["lane_steps"] / max(1, k["warp_steps"]), 2)}
+    return out
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _ref_render_child(q, res, spp, path_length, threads):
     from psychopath_cpp_b200 import scenes
     from oracle import psyref
     ref = psyref.RefScene(scene=scenes.many_light_scene(3, res=res, spp=spp))
-    _, _, rays, secs = ref.render(threads=os.cpu_count() or 1, spp=spp, path_length=path_length, seed=1)
+    _, _, rays, secs = ref.render(threads=threads, spp=spp, path_length=path_length, seed=1)
     q.put((rays, secs))
 
 
-def ref_render_bounded(spp: int, limit_s: float = 240.0):
+def ref_render_bounded(spp: int, limit_s: float = 240.0, threads: int = 0):
     """The reference's render of the frame at `spp` in a child process (spawned,
     so no CUDA state is inherited) with a time limit: a ray with NaN
     differentials makes the reference's patch bisection run without end, so a
@@ -367,7 +404,8 @@ def ref_render_bounded(spp: int, limit_s: float = 240.0):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    p = ctx.Process(target=_ref_render_child, args=(q, RENDER_RES, spp, RENDER_PATH_LENGTH))
+    p = ctx.Process(target=_ref_render_child,
+                    args=(q, RENDER_RES, spp, RENDER_PATH_LENGTH, threads or os.cpu_count() or 1))
     p.start()
     p.join(limit_s)
     if p.is_alive():
@@ -394,10 +432,19 @@ def render_cpu_baseline(spp: int = 4):
         return None
     rays, secs = out
     paths = RENDER_RES[0] * RENDER_RES[1] * spp
-    return {"value": round(paths / secs, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
-            "mrays_per_s": round(rays / secs / 1e6, 3),
-            "sample": "the %dx%d frame at %d spp (%d paths) instead of %d, PathTraceIntegrator::integrate on "
-                      "%d threads" % (RENDER_RES[0], RENDER_RES[1], spp, paths, RENDER_SPP, threads)}
+    res = {"value": round(paths / secs, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
+           "mrays_per_s": round(rays / secs / 1e6, 3), "cpu_model": cpu_model(),
+           "sample": "the %dx%d frame at %d spp (%d paths) instead of %d, PathTraceIntegrator::integrate on "
+                     "%d threads" % (RENDER_RES[0], RENDER_RES[1], spp, paths, RENDER_SPP, threads)}
+    # the same on one core, over the frame at 1 spp
+    one = ref_render_bounded(1, limit_s=300.0, threads=1)
+    if one is not None:
+        p1 = RENDER_RES[0] * RENDER_RES[1]
+        res["one_core"] = {"value": round(p1 / one[1], 1), "unit": "paths/s", "cores": 1,
+                           "mrays_per_s": round(one[0] / one[1] / 1e6, 3),
+                           "sample": "the %dx%d frame at 1 spp (%d paths) on 1 thread" % (RENDER_RES[0],
+                                                                                       RENDER_RES[1], p1)}
+    return res
 
 
 def run_render_reference(args, spp: int = 2):
@@ -424,6 +471,7 @@ def run_render_reference(args, spp: int = 2):
             "config": {"workload": render_workload_name(), "sample_paths_per_step": paths},
             "mrays_per_s": round(rays / tot / 1e6, 3),
             "cpu_baseline": {"value": round(value, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
+                             "cpu_model": cpu_model(),
                              "sample": "the %dx%d frame at %d spp per step (%d paths), PathTraceIntegrator::"
                                        "integrate on %d threads" % (RENDER_RES[0], RENDER_RES[1], spp, paths,
                                                                     threads)},
@@ -507,6 +555,17 @@ def run_batch_ours(args, rank, local, pg, world):
         plain_pass()
     plain_ms = timed(plain_pass, args.steps)
     log("batch: plain pass %.1f ms" % plain_ms)
+    # each render alone (one pass, CUDA events around each), so that the
+    # plain rate can be taken over any subset of the renders
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in entries]
+    for (a, z), it, (x, c) in zip(ev, integs, films):
+        a.record(stream)
+        it.integrate_device(x, c, sp, with_stats=False)
+        z.record(stream)
+    torch.cuda.synchronize(dev)
+    per_render_ms = [a.elapsed_time(z) for a, z in ev]
+    per_render_paths = [e["width"] * e["height"] * e["spp"] for e in entries]
     owner = api.Context(local)
     b = api.BatchRenderer(owner, entries, use_graph=False)
     tune = b.autotune(spp_divisor=16)
@@ -533,6 +592,7 @@ def run_batch_ours(args, rank, local, pg, world):
                                "4 segments", "paths_per_step": paths, "tuned": tune,
                    "l2": "per-wave path state larger than L2"},
         "plain_paths_per_s": round(plain_value, 1), "plain_ms_per_step": round(plain_ms, 3),
+        "plain_per_render": {"ms": [round(x, 3) for x in per_render_ms], "paths": per_render_paths},
         "batched_over_plain": round(value / plain_value, 3), "mrays_per_s": round(rays / (batch_ms * 1e-3) / 1e6, 2),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 5), "traffic": None, "peak_source": peak_kind,
@@ -616,7 +676,8 @@ def batch_cpu_baseline():
         return None
     threads = os.cpu_count() or 1
     return {"value": round(paths / secs, 1), "unit": "paths/s", "cores": threads, "kind": "reference",
-            "mrays_per_s": round(rays / secs / 1e6, 3), "sample": _batch_sample(threads, skipped)}
+            "mrays_per_s": round(rays / secs / 1e6, 3), "sample": _batch_sample(threads, skipped),
+            "left_out": list(skipped), "cpu_model": cpu_model()}
 
 
 def run_batch_reference(args):
@@ -731,6 +792,24 @@ def run_adjoint_ours(args, rank, local, pg, world):
     }
 
 
+def render_line_extras(args, rank, local, pg, world) -> dict:
+    """The other two figures of the headline metric, measured after the
+    render's timed region, each with its own CUDA events and clock record:
+    batched over plain paths/s (48 renders) and adjoint over forward time."""
+    small = argparse.Namespace(**vars(args))
+    small.steps, small.warmup = 1, 1
+    out = {}
+    b = run_batch_ours(small, rank, local, pg, world)
+    out["batched_over_plain"] = {"value": b["batched_over_plain"], "batched_paths_per_s": b["value"],
+                                 "plain_paths_per_s": b["plain_paths_per_s"], "workload": b["config"]["workload"],
+                                 "steps": 1, "clocks": b["clocks"]}
+    small.steps, small.warmup = 10, 3
+    a = run_adjoint_ours(small, rank, local, pg, world)
+    out["adjoint_over_forward"] = {"value": a["value"], "forward_ms": a["forward_ms"], "adjoint_ms": a["adjoint_ms"],
+                                   "workload": a["config"]["workload"], "steps": 10, "clocks": a["clocks"]}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -740,6 +819,8 @@ def main():
     ap.add_argument("--stream-paths", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="render workload: leave out the batched/plain and adjoint/forward figures")
     ap.add_argument("--render-size", default="",
                     help="WxHxSPP: a smaller frame of the render workload (profiling captures); not a bench line")
     args = ap.parse_args()
@@ -760,6 +841,8 @@ def main():
         return
     if args.workload == "render":
         res = run_render_ours(args, rank, local, pg, world)
+        if world == 1 and not args.no_extras and not args.render_size:
+            res.update(render_line_extras(args, rank, local, pg, world))
     elif args.workload == "batch":
         res = run_batch_ours(args, rank, local, pg, world)
     elif args.workload == "adjoint":
@@ -770,6 +853,13 @@ def main():
         if world == 1 and not args.no_cpu_baseline and args.workload in ("render", "trace", "batch"):
             res["cpu_baseline"] = {"render": render_cpu_baseline, "trace": trace_cpu_baseline,
                                    "batch": batch_cpu_baseline}[args.workload]()
+            cb = res["cpu_baseline"]
+            if args.workload == "batch" and cb and cb.get("left_out"):
+                # the plain GPU rate over the renders the reference sample kept
+                pr = res["plain_per_render"]
+                keep = [i for i in range(len(pr["ms"])) if i not in cb["left_out"]]
+                res["plain_paths_per_s_reference_subset"] = round(
+                    sum(pr["paths"][i] for i in keep) / (sum(pr["ms"][i] for i in keep) * 1e-3), 1)
         print(json.dumps(res))
     if pg:
         pg.barrier()

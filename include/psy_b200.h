@@ -233,15 +233,18 @@ int psy_trace_host(psy_ctx* ctx, const psy_ray_soa* rays, uint32_t n, const psy_
  * holds all free device memory, or one whose other streams must not be
  * stalled by the device-wide synchronisation cudaMalloc / cudaFree can
  * cause).  The rays and hits are staged in one fixed-size device array
- * compiled into the library (about 17 MB, reserved when the library's device
- * code is loaded) instead of the context's growable scratch buffers.  Same
- * arguments and results as psy_trace_host, on `stream` (NULL = default
- * stream), synchronised before return.
+ * compiled into the library (about 17 MB per device) instead of the
+ * context's growable scratch buffers.  Same arguments and results as
+ * psy_trace_host, on `stream` (NULL = default stream), synchronised before
+ * return.
  *  - n > PSY_NOALLOC_MAX_RAYS fails with PSY_ERR_ARG before any device work.
  *  - The array is one per device, shared by all contexts: calls that overlap
  *    in time on one device race on it; serialise them.
- *  - The first call on each device resolves the array's address; make it
- *    before any stream capture begins on that device.
+ *  - The array is made resident on a device (its module loaded, its address
+ *    resolved) by psy_ctx_create on that device, or by a call with n == 0,
+ *    which does only that.  Create the context, or make that call, before a
+ *    pool allocator takes the device's free memory and before any stream
+ *    capture begins on that device.
  *  - No device or pinned memory is allocated; only a failing call may grow
  *    the context's error message string.
  */
@@ -317,13 +320,30 @@ int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* 
 /*
  * Optional timing of the traversal kernels, for roofline reports (no
  * counterpart in the reference).  While enabled, psy_render records CUDA
- * events on its stream around each traversal launch (the first
- * PSY_PROFILE_MAX_LAUNCHES since the last read); psy_profile_read waits for
- * them and returns their summed time and count, then starts a new count.
+ * events on its stream around every traversal launch (the event pool starts
+ * at PSY_PROFILE_MAX_LAUNCHES launches and grows as needed);
+ * psy_profile_read waits for them and returns their summed time and count,
+ * then starts a new count.
  */
 #define PSY_PROFILE_MAX_LAUNCHES 4096
 int psy_profile_enable(psy_ctx* ctx, int on);
 int psy_profile_read(psy_ctx* ctx, double* trace_ms, uint32_t* launches);
+
+/*
+ * Work counters of the traversal kernels over the last psy_render,
+ * psy_render_diff or psy_render_adjoint call on ctx, for closest-hit and
+ * occlusion rays (no counterpart in the reference; always collected).
+ * Synchronises the device.  Either pointer may be NULL.
+ */
+typedef struct psy_trace_counters {
+	uint64_t rays;              /* rays traced */
+	uint64_t node_visits;       /* BVH4 inner nodes visited */
+	uint64_t leaf_visits;       /* leaves visited: assembly instance entries and object tests */
+	uint64_t patch_iterations;  /* patch bisection iterations (a leaf test or a split each) */
+	uint64_t warp_steps;        /* traversal warp-loop iterations that ran work */
+	uint64_t lane_steps;        /* lanes that ran work, summed over those iterations (of 32 each) */
+} psy_trace_counters;
+int psy_profile_counters(psy_ctx* ctx, psy_trace_counters* closest, psy_trace_counters* occlusion);
 
 /* ------------------------------------------------------------------ */
 /* Differentiable rendering: parameters and the path-replay adjoint     */
@@ -336,6 +356,11 @@ int psy_profile_read(psy_ctx* ctx, double* trace_ms, uint32_t* launches);
  *      a(lambda) = sum_k params[p+k] * exp(-(lambda - c_k)^2 / (2 s^2)),
  *    c_k = PSY_ALBEDO_BASIS_C0 + k * PSY_ALBEDO_BASIS_STEP nm, s = PSY_ALBEDO_BASIS_SIGMA nm
  *    (the RGB colour's upsampled spectrum is used where shader_param is -1);
+ *  - a Lambert shader with shader_scale_param[s] = q >= 0 keeps its RGB
+ *    colour's upsampled spectrum, scaled by params[q] (the reference's
+ *    spectral upsampling is linear in the colour's magnitude, so this is the
+ *    reference's albedo with the colour scaled by params[q]); a shader takes
+ *    basis weights or a scale, not both;
  *  - a sphere light with object_param[o] = q >= 0 has its emission scaled
  *    by params[q].  Light selection keeps the uploaded energies, so the
  *    estimator stays unbiased for any scale.
@@ -353,6 +378,8 @@ typedef struct psy_diff_desc {
 	const int32_t* shader_param;      /* host: first albedo weight of each shader, or -1 */
 	uint32_t object_count;            /* entries of object_param: the scene's object count */
 	const int32_t* object_param;      /* host: emission scale of each light object, or -1 */
+	uint32_t shader_scale_count;      /* entries of shader_scale_param: 0 (none) or the scene's shader count */
+	const int32_t* shader_scale_param;/* host: the scale of each shader's RGB albedo, or -1 */
 } psy_diff_desc;
 
 /* psy_render with the parameterised colours (same film semantics). */

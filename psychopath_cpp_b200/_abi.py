@@ -25,6 +25,22 @@ PSY_INSTANCE_OBJECT, PSY_INSTANCE_ASSEMBLY = 0, 1
 PSY_SHADER_LAMBERT, PSY_SHADER_EMIT, PSY_SHADER_GTR = 0, 1, 2
 PSY_RAY_CAMERA, PSY_RAY_DIFFUSE, PSY_RAY_OCCLUSION = 1, 2, 32
 
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "psy_b200.h")
+
+
+def header_define(name: str) -> int:
+    """An integer #define of include/psy_b200.h, read from the header itself
+    so that the binding and the library cannot disagree."""
+    import re
+    with open(HEADER_PATH) as f:
+        m = re.search(r"^#define\s+%s\s+(\d+)u?\b" % re.escape(name), f.read(), re.M)
+    if not m:
+        raise KeyError(name)
+    return int(m.group(1))
+
+
+PSY_NOALLOC_MAX_RAYS = header_define("PSY_NOALLOC_MAX_RAYS")
+
 fp = C.POINTER(C.c_float)
 u8p = C.POINTER(C.c_uint8)
 u16p = C.POINTER(C.c_uint16)
@@ -96,7 +112,8 @@ class RenderDesc(C.Structure):
 class DiffDesc(C.Structure):
     _fields_ = [("param_count", C.c_uint32), ("params", C.POINTER(C.c_float)), ("shader_count", C.c_uint32),
                 ("shader_param", C.POINTER(C.c_int32)), ("object_count", C.c_uint32),
-                ("object_param", C.POINTER(C.c_int32))]
+                ("object_param", C.POINTER(C.c_int32)), ("shader_scale_count", C.c_uint32),
+                ("shader_scale_param", C.POINTER(C.c_int32))]
 
 
 class BatchDesc(C.Structure):
@@ -114,11 +131,19 @@ class RenderStats(C.Structure):
                 ("occlusion_rays", C.c_uint64)]
 
 
+class TraceCounters(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("node_visits", C.c_uint64), ("leaf_visits", C.c_uint64),
+                ("patch_iterations", C.c_uint64), ("warp_steps", C.c_uint64), ("lane_steps", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
 # every symbol declared in include/psy_b200.h
 EXPORTED = ["psy_ctx_create", "psy_ctx_destroy", "psy_last_error", "psy_version", "psy_scene_upload",
             "psy_scene_stats_get", "psy_build_bvh4", "psy_build_light_tree", "psy_trace", "psy_trace_host", "psy_sync",
             "psy_trace_host_noalloc", "psy_render_batch", "psy_batch_autotune", "psy_render_diff",
-            "psy_render_adjoint", "psy_profile_enable", "psy_profile_read",
+            "psy_render_adjoint", "psy_profile_enable", "psy_profile_read", "psy_profile_counters",
             "psy_light_sample", "psy_render"]
 
 _lib = None
@@ -147,6 +172,8 @@ def load():
     if hasattr(L, "psy_profile_enable"):
         L.psy_profile_enable.argtypes = [C.c_void_p, C.c_int]
         L.psy_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]
+    if hasattr(L, "psy_profile_counters"):
+        L.psy_profile_counters.argtypes = [C.c_void_p, C.POINTER(TraceCounters), C.POINTER(TraceCounters)]
     if hasattr(L, "psy_render_diff"):
         L.psy_render_diff.argtypes = [C.c_void_p, C.POINTER(RenderDesc), C.POINTER(DiffDesc), C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p]

@@ -184,6 +184,13 @@ class Context:
     def sync(self, stream=None):
         self.check(self.L.psy_sync(self.h, stream))
 
+    def trace_counters(self) -> dict:
+        """Traversal work counters of the last render on this context
+        (psy_profile_counters): {"closest": {...}, "occlusion": {...}}."""
+        c, o = _abi.TraceCounters(), _abi.TraceCounters()
+        self.check(self.L.psy_profile_counters(self.h, C.byref(c), C.byref(o)))
+        return {"closest": c.as_dict(), "occlusion": o.as_dict()}
+
 
 def _check(L, rc: int, what: str):
     if rc != 0:
@@ -267,17 +274,19 @@ class Tracer:
 
     def trace_noalloc(self, rays: dict, fields=("hit", "id", "t", "uv"), stream=None) -> Dict[str, np.ndarray]:
         """psy_trace_host_noalloc: as trace(), staged in the library's
-        fixed-size device array (at most NOALLOC_MAX_RAYS rays per call)."""
+        fixed-size device array (at most _abi.PSY_NOALLOC_MAX_RAYS rays per
+        call).  fields=None passes no hit arrays at all (hits = NULL)."""
         n = len(rays["time"])
         rs, keep = _ray_soa_host(rays)
         out = {}
         hs = _abi.HitSoA()
-        for f in fields:
+        for f in fields or ():
             dt, w = HIT_FIELDS[f]
             arr = np.zeros((n, w) if w > 1 else (n,), dt)
             out[f] = arr
             setattr(hs, f, arr.ctypes.data_as(C.c_void_p))
-        self.ctx.check(self.ctx.L.psy_trace_host_noalloc(self.ctx.h, C.byref(rs), n, C.byref(hs), stream))
+        self.ctx.check(self.ctx.L.psy_trace_host_noalloc(self.ctx.h, C.byref(rs), n,
+                                                         C.byref(hs) if fields is not None else None, stream))
         return out
 
     def trace_device(self, rays: dict, hits: dict, stream=None) -> None:
@@ -461,22 +470,27 @@ class DiffRenderer:
     path-replay adjoint (psy_render_adjoint).  shader_param / object_param
     map scene shaders and objects (flat_indices order) to parameter indices
     (-1 = fixed): a shader gets 4 albedo basis weights, a light one emission
-    scale."""
+    scale.  shader_scale_param (optional) instead gives a shader one
+    parameter that scales its RGB albedo."""
 
     def __init__(self, ctx: Context, width: int, height: int, spp: int, shader_param, object_param,
-                 param_count: int, seed: int = 1, path_length: int = 4, stream_paths: int = 0):
+                 param_count: int, seed: int = 1, path_length: int = 4, stream_paths: int = 0,
+                 shader_scale_param=None):
         self.ctx = ctx
         self.desc = _abi.RenderDesc(width, height, spp, seed, path_length, stream_paths, 0)
         self.param_count = int(param_count)
         self._sp = np.ascontiguousarray(np.asarray(shader_param, np.int32))
         self._op = np.ascontiguousarray(np.asarray(object_param, np.int32))
+        self._ss = (np.ascontiguousarray(np.asarray(shader_scale_param, np.int32))
+                    if shader_scale_param is not None else np.zeros(0, np.int32))
         self.stats = _abi.RenderStats()
 
     def _diff(self, params) -> _abi.DiffDesc:
         assert params.dtype == _torch().float32 and params.is_cuda and params.numel() == self.param_count
         return _abi.DiffDesc(self.param_count, C.cast(C.c_void_p(params.data_ptr()), _abi.fp),
                              len(self._sp), self._sp.ctypes.data_as(C.POINTER(C.c_int32)),
-                             len(self._op), self._op.ctypes.data_as(C.POINTER(C.c_int32)))
+                             len(self._op), self._op.ctypes.data_as(C.POINTER(C.c_int32)),
+                             len(self._ss), self._ss.ctypes.data_as(C.POINTER(C.c_int32)))
 
     def forward(self, params, xyz=None, counts=None, stream=None, with_stats: bool = False):
         """Film sums (h*w*3) and counts (h*w) of one render, as device tensors."""

@@ -114,4 +114,6 @@ def main(path: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/color/spectra_xyz_5nm_380_780_0.97.h")
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_spectral_table.py <reference>/color/spectra_xyz_5nm_380_780_0.97.h")
+    main(sys.argv[1])

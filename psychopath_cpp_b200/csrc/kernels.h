@@ -48,7 +48,8 @@ struct RenderParams {
 	uint32_t* counts;        // film sample counts (may be null)
 	// differentiable rendering (all null in plain renders)
 	const float* params;     // parameter vector
-	const int* shader_param; // per scene shader: first of its 4 albedo weights, or -1
+	const int* shader_param; // per scene shader: first of its 4 albedo weights (>= 0), -2 - q for an RGB
+	                         // albedo scaled by params[q], or -1
 	const int* object_param; // per scene object: its emission scale, or -1
 	const float* dl_dxyz;    // adjoint: dL / d(film sums), width * height * 3
 	float* grad;             // adjoint: gradient accumulator, param_count floats
@@ -87,6 +88,9 @@ struct PathSoA {
 	float4* valb;       // albedo spectrum of each parameterised vertex, PSY_ADJ_MAX_VERTS per path
 	int* vpid;          // its first albedo weight (-1: not parameterised), PSY_ADJ_MAX_VERTS per path
 	int* nee_param;     // emission scale of the light sampled at the current vertex, or -1
+	float4* vdsc;       // d(albedo)/d(scale) of each scale-parameterised vertex, PSY_ADJ_MAX_VERTS per path
+	float4* fexcl;      // fcol with every parameterised albedo factor left out
+	float4* nee_base;   // the pending light contribution with its parameterised factors left out
 };
 
 // Rays and hits of a wave by queue position (cap = the wave's path capacity).
@@ -98,11 +102,23 @@ struct WaveBufs {
 	int cap;
 };
 
+// Traversal counters of a render, one block of TC_COUNT per ray kind
+// (closest-hit rays first, then occlusion rays), summed over its launches.
+enum : int {
+	TC_RAYS = 0,        // rays traced
+	TC_NODES = 1,       // BVH4 inner nodes visited
+	TC_LEAVES = 2,      // leaves visited (assembly instance entries and object tests)
+	TC_PATCH_ITERS = 3, // patch bisection loop iterations (leaf tests and splits)
+	TC_WARP_STEPS = 4,  // traversal warp-loop iterations that ran work
+	TC_LANE_STEPS = 5,  // lanes that ran work, summed over those iterations
+	TC_COUNT = 8
+};
+
 struct WaveQueues {
 	int* q0;
 	int* q1;
 	int* counters;      // render_counter_count(path_length) work and live counters
-	unsigned long long* rays;   // [0] closest-hit rays traced, [1] occlusion rays traced
+	unsigned long long* rays;   // 2 * TC_COUNT traversal counters: closest-hit rays, then occlusion rays
 };
 
 // Optional profiling: CUDA events recorded around each traversal launch, in

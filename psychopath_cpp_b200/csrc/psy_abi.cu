@@ -114,6 +114,12 @@ static int check_render(psy_ctx* ctx, const psy_render_desc* desc, const char* w
 	if (desc->path_length > 40) return ctx_fail(ctx, PSY_ERR_ARG, "%s: path_length must be at most 40", who);
 	if (ctx->host->assemblies[0].light_root < 0)
 		return ctx_fail(ctx, PSY_ERR_ARG, "%s: the scene has no lights (the reference integrator needs one)", who);
+	// The trace reports GTR closures (Intersection::surface_closure), but the
+	// wave kernels shade Lambert and emission only: refuse rather than end
+	// such paths early.
+	for (size_t i = 0; i < ctx->host->shaders.size(); ++i)
+		if (ctx->host->shaders[i].kind == SHADER_GTR)
+			return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader %zu is GTR, which the renderer does not shade", who, i);
 	return PSY_OK;
 }
 
@@ -176,18 +182,25 @@ static int wave_set(psy_ctx* ctx, const char* prefix, uint64_t P, uint32_t path_
 	ps.valb = nullptr;
 	ps.vpid = nullptr;
 	ps.nee_param = nullptr;
+	ps.vdsc = nullptr;
+	ps.fexcl = nullptr;
+	ps.nee_base = nullptr;
 	if (adjoint) {
 		ps.adj = (float4*)buf("adj", P * 16);
 		ps.valb = (float4*)buf("valb", P * 16 * PSY_ADJ_MAX_VERTS);
 		ps.vpid = (int*)buf("vpid", P * 4 * PSY_ADJ_MAX_VERTS);
 		ps.nee_param = (int*)buf("neep", P * 4);
-		if (!ps.adj || !ps.valb || !ps.vpid || !ps.nee_param) return rc ? rc : PSY_ERR_OOM;
+		ps.vdsc = (float4*)buf("vdsc", P * 16 * PSY_ADJ_MAX_VERTS);
+		ps.fexcl = (float4*)buf("fexcl", P * 16);
+		ps.nee_base = (float4*)buf("neeb", P * 16);
+		if (!ps.adj || !ps.valb || !ps.vpid || !ps.nee_param || !ps.vdsc || !ps.fexcl || !ps.nee_base)
+			return rc ? rc : PSY_ERR_OOM;
 	}
 	WaveQueues& wq = ws->wq;
 	wq.q0 = (int*)buf("q0", P * 4);
 	wq.q1 = (int*)buf("q1", P * 4);
 	wq.counters = (int*)buf("counters", sizeof(int) * render_counter_count(path_length));
-	wq.rays = (unsigned long long*)buf("rays", 2 * sizeof(unsigned long long));
+	wq.rays = (unsigned long long*)buf("rays", 2 * TC_COUNT * sizeof(unsigned long long));
 	WaveBufs& wb = ws->wb;
 	wb.cap = (int)P;
 	wb.ray[0] = (float4*)buf("ray0", P * 80);
@@ -199,6 +212,30 @@ static int wave_set(psy_ctx* ctx, const char* prefix, uint64_t P, uint32_t path_
 	    !ps.hit || !ps.pray || !ps.sample || !ps.rid || !wq.q0 || !wq.q1 || !wq.counters || !wq.rays || !wb.ray[0] ||
 	    !wb.ray[1] || !wb.hit_f || !wb.hit_i || !wb.occl)
 		return rc ? rc : PSY_ERR_OOM;
+	return PSY_OK;
+}
+
+// Profiling: makes room for `pairs` more traversal-launch timings.  The
+// event pool grows as needed, so every launch of the profiled region is
+// timed.
+static int timer_reserve(psy_ctx* ctx, int pairs) {
+	const size_t need = 2 * (size_t)(ctx->timer_used + pairs);
+	if (ctx->timer_events.size() < need) {
+		size_t n = ctx->timer_events.size();
+		size_t cap = n ? n : 2 * (size_t)PSY_PROFILE_MAX_LAUNCHES;
+		while (cap < need) cap *= 2;
+		ctx->timer_events.resize(cap, nullptr);
+		for (size_t k = n; k < cap; ++k) {
+			const int rc = ctx_cuda(ctx, cudaEventCreate(&ctx->timer_events[k]), "profiling: event");
+			if (rc) {
+				ctx->timer_events.resize(k);
+				return rc;
+			}
+		}
+	}
+	ctx->timer.events = ctx->timer_events.data();
+	ctx->timer.capacity = (int)(ctx->timer_events.size() / 2);
+	ctx->timer.used = &ctx->timer_used;
 	return PSY_OK;
 }
 
@@ -216,9 +253,13 @@ static int render_single(psy_ctx* ctx, const psy_render_desc* desc, const Render
 	if (P > total) P = total;
 	WaveSet ws;
 	if ((rc = wave_set(ctx, "r_", P, rp.path_length, &ws, adjoint))) return rc;
-	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, 2 * sizeof(unsigned long long), st), "memset"))) return rc;
+	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, 2 * TC_COUNT * sizeof(unsigned long long), st), "memset")))
+		return rc;
+	ctx->last_counts = ws.wq.rays;
 	uint32_t launches = 0, waves = 0;
 	for (uint64_t base = 0; base < total; base += P) {
+		// each wave launches 2 * path_length traversal kernels
+		if (ctx->profiling && (rc = timer_reserve(ctx, 2 * (int)rp.path_length))) return rc;
 		WaveRange wv;
 		wv.base = base;
 		wv.paths = (int)((total - base) < P ? (total - base) : P);
@@ -233,13 +274,13 @@ static int render_single(psy_ctx* ctx, const psy_render_desc* desc, const Render
 		++waves;
 	}
 	if (stats) {
-		unsigned long long rays[2] = {0, 0};
-		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(rays, ws.wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
+		unsigned long long cnt[2 * TC_COUNT] = {};
+		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(cnt, ws.wq.rays, sizeof(cnt), cudaMemcpyDeviceToHost, st), "D2H")))
 			return rc;
 		if ((rc = ctx->check_status(st))) return rc;
 		stats->paths = total;
-		stats->rays = rays[0] + rays[1];
-		stats->occlusion_rays = rays[1];
+		stats->rays = cnt[TC_RAYS] + cnt[TC_COUNT + TC_RAYS];
+		stats->occlusion_rays = cnt[TC_COUNT + TC_RAYS];
 		stats->launches = launches;
 		stats->waves = waves;
 	}
@@ -255,14 +296,25 @@ static int diff_params(psy_ctx* ctx, const psy_diff_desc* d, const char* who, Re
 		return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader_param must have one entry per scene shader (%zu)", who, ns);
 	if (d->object_count != no || (no && !d->object_param))
 		return ctx_fail(ctx, PSY_ERR_ARG, "%s: object_param must have one entry per scene object (%zu)", who, no);
+	if (d->shader_scale_count != 0 && (d->shader_scale_count != ns || !d->shader_scale_param))
+		return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader_scale_param must be empty or have one entry per scene shader (%zu)",
+		                who, ns);
 	const int pc = (int)d->param_count;
+	// one device entry per shader: weights (>= 0), a scale q (-2 - q), or none (-1)
+	std::vector<int> code(ns, -1);
 	for (size_t i = 0; i < ns; ++i) {
 		const int p = d->shader_param[i];
+		const int q = d->shader_scale_count ? d->shader_scale_param[i] : -1;
 		if (p < -1 || (p >= 0 && p + 3 >= pc))
 			return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader %zu's albedo weights %d..%d are outside the %d parameters", who,
 			                i, p, p + 3, pc);
-		if (p >= 0 && ctx->host->shaders[i].kind != SHADER_LAMBERT)
+		if (q < -1 || q >= pc)
+			return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader %zu's albedo scale %d is out of range", who, i, q);
+		if (p >= 0 && q >= 0)
+			return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader %zu has both basis weights and a scale", who, i);
+		if ((p >= 0 || q >= 0) && ctx->host->shaders[i].kind != SHADER_LAMBERT)
 			return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader %zu is not Lambert", who, i);
+		code[i] = p >= 0 ? p : (q >= 0 ? -2 - q : -1);
 	}
 	for (size_t i = 0; i < no; ++i) {
 		const int p = d->object_param[i];
@@ -275,7 +327,7 @@ static int diff_params(psy_ctx* ctx, const psy_diff_desc* d, const char* who, Re
 	if (!sp) return rc;
 	int* op = static_cast<int*>(ctx->scratch_buffer("d_opar", sizeof(int) * (no ? no : 1), &rc));
 	if (!op) return rc;
-	if (ns && (rc = ctx_cuda(ctx, cudaMemcpy(sp, d->shader_param, sizeof(int) * ns, cudaMemcpyHostToDevice), who)))
+	if (ns && (rc = ctx_cuda(ctx, cudaMemcpy(sp, code.data(), sizeof(int) * ns, cudaMemcpyHostToDevice), who)))
 		return rc;
 	if (no && (rc = ctx_cuda(ctx, cudaMemcpy(op, d->object_param, sizeof(int) * no, cudaMemcpyHostToDevice), who)))
 		return rc;
@@ -337,7 +389,8 @@ static int render_batch(psy_ctx* ctx, const psy_batch_desc* b, psy_render_stats*
 	                                        st),
 	                   "psy_render_batch: render table")))
 		return rc;
-	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, 2 * sizeof(unsigned long long), st), "memset"))) return rc;
+	if ((rc = ctx_cuda(ctx, cudaMemsetAsync(ws.wq.rays, 0, 2 * TC_COUNT * sizeof(unsigned long long), st), "memset")))
+		return rc;
 	// waves on pixel boundaries
 	std::vector<WaveRange> waves;
 	{
@@ -431,13 +484,13 @@ static int render_batch(psy_ctx* ctx, const psy_batch_desc* b, psy_render_stats*
 		if ((rc = launch_all(st))) return rc;
 	}
 	if (stats) {
-		unsigned long long rays[2] = {0, 0};
-		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(rays, ws.wq.rays, sizeof(rays), cudaMemcpyDeviceToHost, st), "D2H")))
+		unsigned long long cnt[2 * TC_COUNT] = {};
+		if ((rc = ctx_cuda(ctx, cudaMemcpyAsync(cnt, ws.wq.rays, sizeof(cnt), cudaMemcpyDeviceToHost, st), "D2H")))
 			return rc;
 		if ((rc = ctx->check_status(st))) return rc;
 		stats->paths = total;
-		stats->rays = rays[0] + rays[1];
-		stats->occlusion_rays = rays[1];
+		stats->rays = cnt[TC_RAYS] + cnt[TC_COUNT + TC_RAYS];
+		stats->occlusion_rays = cnt[TC_COUNT + TC_RAYS];
 		stats->launches = launches;
 		stats->waves = (uint32_t)waves.size();
 	}
@@ -484,6 +537,18 @@ int psy_ctx_create(int device, psy_ctx** out) {
 		ctx->halton.cmul = static_cast<const double*>(p2);
 	}
 	ctx->ident_inv = reference_identity_inverse_scale();
+	{
+		const HostRcp& hr = host_rcp();
+		void* p = nullptr;
+		const size_t bytes = hr.entries.size() * sizeof(uint32_t);
+		if (cudaMalloc(&p, bytes) != cudaSuccess) return PSY_ERR_OOM;
+		ctx->const_allocs.push_back(p);
+		if (cudaMemcpy(p, hr.entries.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) return PSY_ERR_DEVICE;
+		ctx->rcp = RcpTable{static_cast<const uint32_t*>(p), hr.shift};
+	}
+	// the fixed array of psy_trace_host_noalloc is reserved now, so that its
+	// first call allocates nothing
+	if (noalloc_reserve(ctx.get()) != PSY_OK) return PSY_ERR_OOM;
 	*out = ctx.release();
 	return PSY_OK;
 }
@@ -524,6 +589,7 @@ int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* desc) {
 	UP(cam_focus, b->cam_focus);
 #undef UP
 	d.assembly_count = (int)b->assemblies.size();
+	d.rcp = ctx->rcp;
 	d.max_depth = b->max_depth;
 	d.features = b->features;
 	d.dice_rate = b->dice_rate;
@@ -880,18 +946,36 @@ int psy_batch_autotune(psy_ctx* ctx, const psy_batch_desc* b, uint32_t spp_divis
 int psy_profile_enable(psy_ctx* ctx, int on) {
 	if (!ctx) return PSY_ERR_ARG;
 	cudaSetDevice(ctx->device);
-	if (on && ctx->timer_events.empty()) {
-		ctx->timer_events.resize(2 * (size_t)PSY_PROFILE_MAX_LAUNCHES);
-		for (cudaEvent_t& e : ctx->timer_events) {
-			int rc = ctx_cuda(ctx, cudaEventCreate(&e), "psy_profile_enable: event");
-			if (rc) return rc;
-		}
-		ctx->timer.events = ctx->timer_events.data();
-		ctx->timer.capacity = PSY_PROFILE_MAX_LAUNCHES;
-		ctx->timer.used = &ctx->timer_used;
-	}
 	ctx->timer_used = 0;
+	if (on) {
+		const int rc = timer_reserve(ctx, PSY_PROFILE_MAX_LAUNCHES);
+		if (rc) return rc;
+	}
 	ctx->profiling = on != 0;
+	return PSY_OK;
+}
+
+int psy_profile_counters(psy_ctx* ctx, psy_trace_counters* closest, psy_trace_counters* occlusion) {
+	if (!ctx) return PSY_ERR_ARG;
+	if (!ctx->last_counts) return ctx_fail(ctx, PSY_ERR_ARG, "psy_profile_counters: no render on this context yet");
+	cudaSetDevice(ctx->device);
+	int rc = ctx_cuda(ctx, cudaDeviceSynchronize(), "psy_profile_counters: synchronize");
+	if (rc) return rc;
+	unsigned long long cnt[2 * TC_COUNT] = {};
+	if ((rc = ctx_cuda(ctx, cudaMemcpy(cnt, ctx->last_counts, sizeof(cnt), cudaMemcpyDeviceToHost),
+	                   "psy_profile_counters: read")))
+		return rc;
+	psy_trace_counters* outs[2] = {closest, occlusion};
+	for (int k = 0; k < 2; ++k) {
+		if (!outs[k]) continue;
+		const unsigned long long* c = cnt + k * TC_COUNT;
+		outs[k]->rays = c[TC_RAYS];
+		outs[k]->node_visits = c[TC_NODES];
+		outs[k]->leaf_visits = c[TC_LEAVES];
+		outs[k]->patch_iterations = c[TC_PATCH_ITERS];
+		outs[k]->warp_steps = c[TC_WARP_STEPS];
+		outs[k]->lane_steps = c[TC_LANE_STEPS];
+	}
 	return PSY_OK;
 }
 

@@ -38,6 +38,7 @@ struct psy_ctx {
 	psy::HaltonDev halton{};
 	std::vector<void*> const_allocs;
 	float ident_inv = 1.0f;
+	psy::RcpTable rcp{};  // device copy of the host CPU's reciprocal table
 	// batched rendering: the instantiated graph of the last batch and the
 	// launch configuration it was captured for, and the autotuner's choice
 	cudaGraphExec_t batch_graph = nullptr;
@@ -50,6 +51,8 @@ struct psy_ctx {
 	std::vector<cudaEvent_t> timer_events;
 	int timer_used = 0;
 	psy::LaunchTimer timer{};
+	// traversal counters of the last psy_render* call (its scratch buffer)
+	const unsigned long long* last_counts = nullptr;
 
 	~psy_ctx();
 	void free_scene();
@@ -63,5 +66,8 @@ struct psy_ctx {
 
 int ctx_fail(psy_ctx* ctx, int code, const char* fmt, ...);
 int ctx_cuda(psy_ctx* ctx, cudaError_t e, const char* what);
+// Makes the fixed trace array of psy_trace_host_noalloc resident on ctx's
+// device (psy_noalloc.cu).
+int noalloc_reserve(psy_ctx* ctx);
 
 #endif

@@ -12,10 +12,11 @@
  *     ("a op b ? a : b") exactly where the reference uses each;
  *   - lerp(alpha, a, b) = a*(1-alpha) + b*alpha (reference utils/utils.hpp:53-56),
  *     lerp_seq as utils/utils.hpp:76-91.
- * The one deliberate difference: Matrix44::inverse in the reference uses an
- * SSE cofactor inverse with the approximate reciprocal instruction
- * (utils/simd.hpp:110-205), whose last bits depend on the CPU model; here
- * the inverse is the cofactor expansion evaluated in double and rounded.
+ *   - Matrix44::inverse follows the reference's SSE cofactor routine
+ *     (utils/simd.hpp:110-205, after Intel's application note AP-928,
+ *     "Streaming SIMD Extensions - Inverse of 4x4 Matrix") lane for lane, and
+ *     its approximate reciprocal of the determinant is the host CPU's own
+ *     rcpss, tabulated on the host (host_cpu.cpp) and looked up here.
  */
 #ifndef PSY_MATH_H
 #define PSY_MATH_H
@@ -198,55 +199,151 @@ PSY_HD V3 dir_transpose(const M44& t, V3 v) {
 	return V3(r[0], r[1], r[2]);
 }
 
-// Matrix inverse (cofactor expansion in double, rounded to float).  A
-// singular matrix gives an all-NaN matrix, as the reference's does.
-PSY_HD M44 m44_inverse(const M44& a) {
-	double m[16];
-	for (int i = 0; i < 16; ++i) m[i] = (double)a.m[i / 4][i % 4];
-	double inv[16];
-	inv[0] = m[5] * m[10] * m[15] - m[5] * m[11] * m[14] - m[9] * m[6] * m[15] + m[9] * m[7] * m[14] +
-	         m[13] * m[6] * m[11] - m[13] * m[7] * m[10];
-	inv[4] = -m[4] * m[10] * m[15] + m[4] * m[11] * m[14] + m[8] * m[6] * m[15] - m[8] * m[7] * m[14] -
-	         m[12] * m[6] * m[11] + m[12] * m[7] * m[10];
-	inv[8] = m[4] * m[9] * m[15] - m[4] * m[11] * m[13] - m[8] * m[5] * m[15] + m[8] * m[7] * m[13] +
-	         m[12] * m[5] * m[11] - m[12] * m[7] * m[9];
-	inv[12] = -m[4] * m[9] * m[14] + m[4] * m[10] * m[13] + m[8] * m[5] * m[14] - m[8] * m[6] * m[13] -
-	          m[12] * m[5] * m[10] + m[12] * m[6] * m[9];
-	inv[1] = -m[1] * m[10] * m[15] + m[1] * m[11] * m[14] + m[9] * m[2] * m[15] - m[9] * m[3] * m[14] -
-	         m[13] * m[2] * m[11] + m[13] * m[3] * m[10];
-	inv[5] = m[0] * m[10] * m[15] - m[0] * m[11] * m[14] - m[8] * m[2] * m[15] + m[8] * m[3] * m[14] +
-	         m[12] * m[2] * m[11] - m[12] * m[3] * m[10];
-	inv[9] = -m[0] * m[9] * m[15] + m[0] * m[11] * m[13] + m[8] * m[1] * m[15] - m[8] * m[3] * m[13] -
-	         m[12] * m[1] * m[11] + m[12] * m[3] * m[9];
-	inv[13] = m[0] * m[9] * m[14] - m[0] * m[10] * m[13] - m[8] * m[1] * m[14] + m[8] * m[2] * m[13] +
-	          m[12] * m[1] * m[10] - m[12] * m[2] * m[9];
-	inv[2] = m[1] * m[6] * m[15] - m[1] * m[7] * m[14] - m[5] * m[2] * m[15] + m[5] * m[3] * m[14] +
-	         m[13] * m[2] * m[7] - m[13] * m[3] * m[6];
-	inv[6] = -m[0] * m[6] * m[15] + m[0] * m[7] * m[14] + m[4] * m[2] * m[15] - m[4] * m[3] * m[14] -
-	         m[12] * m[2] * m[7] + m[12] * m[3] * m[6];
-	inv[10] = m[0] * m[5] * m[15] - m[0] * m[7] * m[13] - m[4] * m[1] * m[15] + m[4] * m[3] * m[13] +
-	          m[12] * m[1] * m[7] - m[12] * m[3] * m[5];
-	inv[14] = -m[0] * m[5] * m[14] + m[0] * m[6] * m[13] + m[4] * m[1] * m[14] - m[4] * m[2] * m[13] -
-	          m[12] * m[1] * m[6] + m[12] * m[2] * m[5];
-	inv[3] = -m[1] * m[6] * m[11] + m[1] * m[7] * m[10] + m[5] * m[2] * m[11] - m[5] * m[3] * m[10] -
-	         m[9] * m[2] * m[7] + m[9] * m[3] * m[6];
-	inv[7] = m[0] * m[6] * m[11] - m[0] * m[7] * m[10] - m[4] * m[2] * m[11] + m[4] * m[3] * m[10] +
-	         m[8] * m[2] * m[7] - m[8] * m[3] * m[6];
-	inv[11] = -m[0] * m[5] * m[11] + m[0] * m[7] * m[9] + m[4] * m[1] * m[11] - m[4] * m[3] * m[9] -
-	          m[8] * m[1] * m[7] + m[8] * m[3] * m[5];
-	inv[15] = m[0] * m[5] * m[10] - m[0] * m[6] * m[9] - m[4] * m[1] * m[10] + m[4] * m[2] * m[9] +
-	          m[8] * m[1] * m[6] - m[8] * m[2] * m[5];
-	const double det = m[0] * inv[0] + m[1] * inv[4] + m[2] * inv[8] + m[3] * inv[12];
-	if (!(det != 0.0) || !(det - det == 0.0)) return m44_nan();  // zero or non-finite
-	const double idet = 1.0 / det;
-	M44 r;
-	for (int i = 0; i < 16; ++i) r.m[i / 4][i % 4] = (float)(inv[i] * idet);
-	return r;
+// The host CPU's approximate reciprocal instruction (rcpss) as a table.
+// On the x86 cores measured so far its result for a normal input x =
+// m * 2^e depends only on the leading bits of the mantissa m and scales
+// exactly with 2^-e, so `bits[k]` holds the result bits for the input
+// 1 + k / 2^(23 - shift) (shift = 12: 2048 entries); host_cpu.cpp verifies
+// that against the instruction for every mantissa and falls back to the
+// full table (shift 0) on a core where it does not hold.
+struct RcpTable {
+	const uint32_t* bits;
+	int shift;
+};
+
+PSY_HD uint32_t f2u(float f) {
+#if defined(__CUDA_ARCH__)
+	return __float_as_uint(f);
+#else
+	uint32_t u;
+	__builtin_memcpy(&u, &f, 4);
+	return u;
+#endif
+}
+PSY_HD float u2f(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+	return __uint_as_float(u);
+#else
+	float f;
+	__builtin_memcpy(&f, &u, 4);
+	return f;
+#endif
 }
 
-PSY_HD V3 pos_from(const M44& t, V3 v) { return pos_to(m44_inverse(t), v); }
-PSY_HD V3 dir_from(const M44& t, V3 v) { return dir_to(m44_inverse(t), v); }
-PSY_HD V3 nor_to(const M44& t, V3 v) { return dir_transpose(m44_inverse(t), v); }
+// rcpss of x: denormal inputs count as zero (signed infinity), infinities
+// give signed zero, NaN stays NaN, and results below the normal range
+// flush to signed zero, as the instruction does.
+PSY_HD float approx_rcp(float x, const RcpTable& t) {
+	const uint32_t b = f2u(x);
+	const uint32_t sign = b & 0x80000000u;
+	const int e = (int)((b >> 23) & 0xffu);
+	const uint32_t m = b & 0x7fffffu;
+	if (e == 0) return u2f(sign | 0x7f800000u);
+	if (e == 255) return m ? u2f(b | 0x400000u) : u2f(sign);
+	const uint32_t r = t.bits[m >> t.shift];
+	const int re = (int)((r >> 23) & 0xffu) - (e - 127);
+	if (re <= 0) return u2f(sign);
+	return u2f(sign | ((uint32_t)re << 23) | (r & 0x7fffffu));
+}
+
+// Four SSE lanes and the shuffles the inverse uses (_mm_shuffle_ps(a, b,
+// imm): lanes 0, 1 from a, lanes 2, 3 from b, two bits of imm each).
+struct L4 {
+	float v[4];
+};
+PSY_HD L4 l4(float a, float b, float c, float d) {
+	L4 r;
+	r.v[0] = a; r.v[1] = b; r.v[2] = c; r.v[3] = d;
+	return r;
+}
+PSY_HD L4 operator*(const L4& a, const L4& b) { return l4(a.v[0] * b.v[0], a.v[1] * b.v[1], a.v[2] * b.v[2], a.v[3] * b.v[3]); }
+PSY_HD L4 operator+(const L4& a, const L4& b) { return l4(a.v[0] + b.v[0], a.v[1] + b.v[1], a.v[2] + b.v[2], a.v[3] + b.v[3]); }
+PSY_HD L4 operator-(const L4& a, const L4& b) { return l4(a.v[0] - b.v[0], a.v[1] - b.v[1], a.v[2] - b.v[2], a.v[3] - b.v[3]); }
+template <int IMM>
+PSY_HD L4 shuf(const L4& a, const L4& b) {
+	return l4(a.v[IMM & 3], a.v[(IMM >> 2) & 3], b.v[(IMM >> 4) & 3], b.v[(IMM >> 6) & 3]);
+}
+
+// Matrix44::inverse (reference math/matrix.hpp:319-329 over
+// utils/simd.hpp:110-205): the cofactors of the transposed rows in the
+// routine's lane order, the determinant summed as its shuffles pair the
+// lanes, its reciprocal from rcpss refined by one Newton step, every
+// cofactor times that.  A singular matrix comes out all NaN, as there.
+PSY_HD M44 m44_inverse(const M44& a, const RcpTable& rt) {
+	const float* s = &a.m[0][0];
+	L4 row0 = l4(s[0], s[4], s[8], s[12]);
+	L4 row1 = l4(s[9], s[13], s[1], s[5]);
+	L4 row2 = l4(s[2], s[6], s[10], s[14]);
+	L4 row3 = l4(s[11], s[15], s[3], s[7]);
+	L4 tmp1, minor0, minor1, minor2, minor3;
+	tmp1 = row2 * row3;
+	tmp1 = shuf<0xB1>(tmp1, tmp1);
+	minor0 = row1 * tmp1;
+	minor1 = row0 * tmp1;
+	tmp1 = shuf<0x4E>(tmp1, tmp1);
+	minor0 = (row1 * tmp1) - minor0;
+	minor1 = (row0 * tmp1) - minor1;
+	minor1 = shuf<0x4E>(minor1, minor1);
+
+	tmp1 = row1 * row2;
+	tmp1 = shuf<0xB1>(tmp1, tmp1);
+	minor0 = (row3 * tmp1) + minor0;
+	minor3 = row0 * tmp1;
+	tmp1 = shuf<0x4E>(tmp1, tmp1);
+	minor0 = minor0 - (row3 * tmp1);
+	minor3 = (row0 * tmp1) - minor3;
+	minor3 = shuf<0x4E>(minor3, minor3);
+
+	tmp1 = shuf<0x4E>(row1, row1) * row3;
+	tmp1 = shuf<0xB1>(tmp1, tmp1);
+	row2 = shuf<0x4E>(row2, row2);
+	minor0 = (row2 * tmp1) + minor0;
+	minor2 = row0 * tmp1;
+	tmp1 = shuf<0x4E>(tmp1, tmp1);
+	minor0 = minor0 - (row2 * tmp1);
+	minor2 = (row0 * tmp1) - minor2;
+	minor2 = shuf<0x4E>(minor2, minor2);
+
+	tmp1 = row0 * row1;
+	tmp1 = shuf<0xB1>(tmp1, tmp1);
+	minor2 = (row3 * tmp1) + minor2;
+	minor3 = (row2 * tmp1) - minor3;
+	tmp1 = shuf<0x4E>(tmp1, tmp1);
+	minor2 = (row3 * tmp1) - minor2;
+	minor3 = minor3 - (row2 * tmp1);
+
+	tmp1 = row0 * row3;
+	tmp1 = shuf<0xB1>(tmp1, tmp1);
+	minor1 = minor1 - (row2 * tmp1);
+	minor2 = (row1 * tmp1) + minor2;
+	tmp1 = shuf<0x4E>(tmp1, tmp1);
+	minor1 = (row2 * tmp1) + minor1;
+	minor2 = minor2 - (row1 * tmp1);
+
+	tmp1 = row0 * row2;
+	tmp1 = shuf<0xB1>(tmp1, tmp1);
+	minor1 = (row3 * tmp1) + minor1;
+	minor3 = minor3 - (row1 * tmp1);
+	tmp1 = shuf<0x4E>(tmp1, tmp1);
+	minor1 = minor1 - (row3 * tmp1);
+	minor3 = (row1 * tmp1) + minor3;
+
+	L4 det = row0 * minor0;
+	det = shuf<0x4E>(det, det) + det;
+	const float d = det.v[1] + det.v[0];
+	const float r = approx_rcp(d, rt);
+	const float k = (r + r) - (d * (r * r));
+	M44 out;
+	const L4* mi[4] = {&minor0, &minor1, &minor2, &minor3};
+	for (int i = 0; i < 4; ++i)
+		for (int j = 0; j < 4; ++j) out.m[i][j] = k * mi[i]->v[j];
+	if (k == 0.0f) return m44_nan();
+	return out;
+}
+
+PSY_HD V3 pos_from(const M44& t, V3 v, const RcpTable& rt) { return pos_to(m44_inverse(t, rt), v); }
+PSY_HD V3 dir_from(const M44& t, V3 v, const RcpTable& rt) { return dir_to(m44_inverse(t, rt), v); }
+PSY_HD V3 nor_to(const M44& t, V3 v, const RcpTable& rt) { return dir_transpose(m44_inverse(t, rt), v); }
 PSY_HD V3 nor_from(const M44& t, V3 v) { return dir_transpose(t, v); }
 
 // Transform::get_inv_scale (reference math/transform.hpp:108-114).
@@ -315,8 +412,8 @@ PSY_HD bool box_hit(const Box& b, V3 o, V3 dinv, float tmax, float* t0, float* t
 
 // Box corners transformed with pos_to of the inverse (BBox::inverse_transformed,
 // basics/bbox.hpp:227-258).
-PSY_HD Box box_inverse_transformed(const Box& b, const M44& t) {
-	const M44 inv = m44_inverse(t);
+PSY_HD Box box_inverse_transformed(const Box& b, const M44& t, const RcpTable& rt) {
+	const M44 inv = m44_inverse(t, rt);
 	Box r = box_empty();
 	for (int c = 0; c < 8; ++c) {
 		const V3 v((c & 4) ? b.hi.x : b.lo.x, (c & 2) ? b.hi.y : b.lo.y, (c & 1) ? b.hi.z : b.lo.z);

@@ -8,7 +8,7 @@
  * one that keeps other streams busy while it traces small batches
  * (cudaMalloc / cudaFree may synchronise the whole device and stall them).
  * This variant stages everything in one file-scope device array of fixed
- * size instead, reserved when the library's device code is loaded.
+ * size instead.
  *
  * Limits, stated in the header as well:
  *  - at most PSY_NOALLOC_MAX_RAYS rays per call; larger requests fail with
@@ -16,9 +16,13 @@
  *  - the array is one per device and shared by every context on it, so two
  *    calls that overlap in time on the same device (other threads, other
  *    contexts) race on it: callers serialise them;
- *  - the first call on each device resolves the array's address
- *    (cudaGetSymbolAddress, which may load the module); make that first call
- *    before any stream capture begins on that device.
+ *  - the array's address is resolved once per device (cudaGetSymbolAddress).
+ *    With CUDA's lazy module loading that is also when the module holding
+ *    the array is loaded and the array's device memory is reserved, so
+ *    psy_ctx_create does it for its device (noalloc_reserve); a call with
+ *    n == 0 does it as well, as an explicit warm-up.  Either must come before
+ *    the caller's pool allocator takes the free device memory and before any
+ *    stream capture begins on that device.
  * The only part of the array that must start at zero is the status word the
  * kernel ORs its error flags into; each call clears it on its stream before
  * the launch.
@@ -75,15 +79,26 @@ static int scratch_address(psy_ctx* ctx, char** out) {
 	return PSY_OK;
 }
 
+// Resolves the array on ctx's device (current): loads its module, which
+// reserves the array, once per device.  psy_ctx_create calls it.
+int noalloc_reserve(psy_ctx* ctx) {
+	char* base = nullptr;
+	return scratch_address(ctx, &base);
+}
+
 extern "C" int psy_trace_host_noalloc(psy_ctx* ctx, const psy_ray_soa* rays, uint32_t n, const psy_hit_soa* hits,
                                       void* stream) {
 	if (!ctx) return PSY_ERR_ARG;
-	if (!ctx->has_scene) return ctx_fail(ctx, PSY_ERR_NO_SCENE, "psy_trace_host_noalloc: no scene uploaded");
 	if (n > kMaxRays)
 		return ctx_fail(ctx, PSY_ERR_ARG,
 		                "psy_trace_host_noalloc: %u rays exceed the static scratch capacity of %u rays per call",
 		                n, (unsigned)kMaxRays);
-	if (n == 0) return PSY_OK;
+	if (n == 0) {
+		// warm-up form: only makes sure the array is resident on this device
+		const int rc = ctx_cuda(ctx, cudaSetDevice(ctx->device), "psy_trace_host_noalloc: cudaSetDevice");
+		return rc ? rc : noalloc_reserve(ctx);
+	}
+	if (!ctx->has_scene) return ctx_fail(ctx, PSY_ERR_NO_SCENE, "psy_trace_host_noalloc: no scene uploaded");
 	if (!rays || !rays->o || !rays->d || !rays->odx || !rays->ody || !rays->ddx || !rays->ddy || !rays->time)
 		return ctx_fail(ctx, PSY_ERR_ARG, "psy_trace_host_noalloc: incomplete ray arrays");
 	int rc = ctx_cuda(ctx, cudaSetDevice(ctx->device), "psy_trace_host_noalloc: cudaSetDevice");

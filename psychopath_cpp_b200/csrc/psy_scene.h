@@ -139,6 +139,8 @@ struct DevScene {
 	int cam_xform_count, cam_tfov_count, cam_aperture_count, cam_focus_count;
 	float background[3];
 	float pad0;
+	// the host CPU's approximate reciprocal (psy_math.h), for matrix inverses
+	RcpTable rcp;
 };
 
 }  // namespace psy

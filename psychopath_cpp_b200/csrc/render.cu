@@ -110,7 +110,8 @@ struct StoredHit {
 	float t;
 	float bf;           // 1 when the hit was back-facing
 	float col[3];       // closure colour (Lambert)
-	int pid;            // differentiable renders: the shader's first albedo weight, or -1
+	int pid;            // differentiable renders: the shader's first albedo weight (>= 0), -2 - q when its
+	                    // RGB albedo is scaled by params[q], or -1 (not parameterised)
 	V3 d, odx, ody, ddx, ddy;  // previous ray
 };
 
@@ -167,7 +168,7 @@ __device__ void make_stored(const DevScene& sc, const HitRec& rec, const WorldRa
 	if (h.closure != CLOSURE_LAMBERT) return;
 	M44 inv;
 	if (xf) {
-		inv = m44_inverse(space);
+		inv = m44_inverse(space, sc.rcp);
 	} else {
 		inv = m44_identity();
 		for (int i = 0; i < 4; ++i) inv.m[i][i] = ident_inv;
@@ -263,7 +264,13 @@ __device__ __forceinline__ int emission_param(const RenderParams& rp, int obj) {
 // lambert_eval with the albedo taken from parameters when the stored hit's
 // shader has them.
 __device__ __forceinline__ Spec lambert_eval_p(const RenderParams& rp, const StoredHit& sh, V3 out, float wl) {
-	if (sh.pid < 0) return lambert_eval(sh.col, sh.d, out, sh.n, wl);
+	if (sh.pid == -1) return lambert_eval(sh.col, sh.d, out, sh.n, wl);
+	if (sh.pid < -1) {
+		Spec f = lambert_eval(sh.col, sh.d, out, sh.n, wl);
+		const float q = rp.params[-2 - sh.pid];
+		for (int k = 0; k < 4; ++k) f.e[k] *= q;
+		return f;
+	}
 	const float c = lambert_cos(sh.d, out, sh.n);
 	const Spec a = albedo_spec(rp.params + sh.pid, wl);
 	Spec f;
@@ -273,30 +280,54 @@ __device__ __forceinline__ Spec lambert_eval_p(const RenderParams& rp, const Sto
 
 // Adjoint: adds u . dC/dparams for a radiance contribution C (hero
 // wavelengths) whose albedo factors come from vertices 0..nv-1 of the path
-// and whose emission is scaled by params[lp] (lp < 0: none).  C is a
-// product of the vertices' albedos (linear in their weights) and of the
-// emission scale, so each factor's derivative is C divided by that factor
-// times the factor's own derivative.
-__device__ void grad_add(const RenderParams& rp, float* sg, const PathSoA& ps, int slot, int nv, const Spec& C,
+// and whose emission is scaled by params[lp] (lp < 0: none).  C is the
+// product of B (the contribution with every parameterised albedo and the
+// emission scale left out), the parameterised vertices' albedos (each
+// linear in its four weights) and the scale, so the derivative for one
+// factor is the product of all the others: no division, so a factor that
+// is zero (a black albedo, a light scaled to 0) still gets its gradient.
+__device__ void grad_add(const RenderParams& rp, float* sg, const PathSoA& ps, int slot, int nv, const Spec& B,
                          int lp, float wl) {
 	const float4 u4 = ps.adj[slot];
-	const float uc[4] = {u4.x * C.e[0], u4.y * C.e[1], u4.z * C.e[2], u4.w * C.e[3]};
+	const float ub[4] = {u4.x * B.e[0], u4.y * B.e[1], u4.z * B.e[2], u4.w * B.e[3]};
 	float* g = rp.grad_in_smem ? sg : rp.grad;
+	const float scale = lp >= 0 ? rp.params[lp] : 1.0f;
+	if (nv > PSY_ADJ_MAX_VERTS) nv = PSY_ADJ_MAX_VERTS;
+	float a[PSY_ADJ_MAX_VERTS][4];
+	int pid[PSY_ADJ_MAX_VERTS];
+	for (int v = 0; v < nv; ++v) {
+		pid[v] = ps.vpid[slot * PSY_ADJ_MAX_VERTS + v];
+		const float4 a4 = ps.valb[slot * PSY_ADJ_MAX_VERTS + v];
+		a[v][0] = a4.x; a[v][1] = a4.y; a[v][2] = a4.z; a[v][3] = a4.w;
+	}
 	if (lp >= 0) {
-		const float sc = rp.params[lp];
-		if (sc != 0.0f) atomicAdd(g + lp, ((uc[0] + uc[1]) + (uc[2] + uc[3])) / sc);
+		float d = 0.0f;
+		for (int j = 0; j < 4; ++j) {
+			float q = ub[j];
+			for (int v = 0; v < nv; ++v)
+				if (pid[v] != -1) q *= a[v][j];
+			d += q;
+		}
+		atomicAdd(g + lp, d);
 	}
 	for (int v = 0; v < nv; ++v) {
-		const int pid = ps.vpid[slot * PSY_ADJ_MAX_VERTS + v];
-		if (pid < 0) continue;
-		const float4 a4 = ps.valb[slot * PSY_ADJ_MAX_VERTS + v];
-		const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+		if (pid[v] == -1) continue;
 		float q[4];
-		for (int j = 0; j < 4; ++j) q[j] = a[j] != 0.0f ? uc[j] / a[j] : 0.0f;
+		for (int j = 0; j < 4; ++j) {
+			q[j] = ub[j] * scale;
+			for (int o = 0; o < nv; ++o)
+				if (o != v && pid[o] != -1) q[j] *= a[o][j];
+		}
+		if (pid[v] < -1) {
+			// scaled RGB albedo: its derivative is the upsampled colour
+			const float4 u = ps.vdsc[slot * PSY_ADJ_MAX_VERTS + v];
+			atomicAdd(g + (-2 - pid[v]), ((q[0] * u.x + q[1] * u.y) + q[2] * u.z) + q[3] * u.w);
+			continue;
+		}
 		for (int k = 0; k < 4; ++k) {
 			float d = 0.0f;
 			for (int j = 0; j < 4; ++j) d += q[j] * albedo_basis(k, wavelength_n(wl, j));
-			atomicAdd(g + pid + k, d);
+			atomicAdd(g + pid[v] + k, d);
 		}
 	}
 }
@@ -369,6 +400,7 @@ __global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, Wave
 			u[j] = ((g[0] * X_1931(lw) + g[1] * Y_1931(lw)) + g[2] * Z_1931(lw)) * (0.25f * XYZ_NORM_FAC);
 		}
 		ps.adj[slot] = make_float4(u[0], u[1], u[2], u[3]);
+		ps.fexcl[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
 	}
 }
 
@@ -411,12 +443,13 @@ __global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, Wave
 template <class W, unsigned F, bool OCCL>
 __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, const float4* __restrict__ rb,
                                                          const int* n_dev, int n_host, int* work,
-                                                         unsigned long long* ray_count, unsigned* status) {
+                                                         unsigned long long* counts, unsigned* status) {
 	const int n = n_dev ? *n_dev : n_host;
 	const int lane = threadIdx.x & 31;
 	const unsigned lt_mask = (1u << lane) - 1u;
 	unsigned err = 0;
-	unsigned long long rays = 0;
+	// per-lane work counters (TC_*), and the warp's own (lane 0 keeps them)
+	unsigned rays = 0, c_nodes = 0, c_leaves = 0, c_iters = 0, c_warp = 0, c_lanes = 0;
 	TraceState<F> st;
 	int my = -1;    // queue position of this lane's ray, -1 = idle
 	bool at_leaf = false;  // walk_nodes stopped at a leaf (st.leaf)
@@ -460,18 +493,25 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 		}
 		const int cn = __popc(nmask), cl = __popc(lmask) * PSY_LEAF_WEIGHT, cp = __popc(pmask) * PSY_PATCH_WEIGHT;
 		const int run = (cp >= cl && cp >= cn) ? 3 : (cl >= cn) ? 2 : 1;
+		++c_warp;
+		c_lanes += __popc(run == 1 ? nmask : run == 2 ? lmask : pmask);
 		bool live = true;
 		if (kind == run) {
 			const DevScene& sc = w.scene(rid);
 			if (run == 1) {
-				const int r = walk_nodes<F>(sc, st, PSY_WALK_NODES);
+				int left = PSY_WALK_NODES;
+				const int r = walk_nodes<F>(sc, st, left);
+				c_nodes += PSY_WALK_NODES - left;
 				live = r != WALK_DONE;
 				at_leaf = r == WALK_LEAF;
 			} else if (run == 2) {
 				at_leaf = false;
+				++c_leaves;
 				live = leaf_visit<F>(sc, st);
 			} else {
-				live = patch_step<F>(sc, st, PSY_PATCH_UNITS);
+				int left = PSY_PATCH_UNITS;
+				live = patch_step<F>(sc, st, left);
+				c_iters += PSY_PATCH_UNITS - left;
 			}
 		}
 		if (!live) {
@@ -481,8 +521,18 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 			my = -1;
 		}
 	}
-	for (int o = 16; o > 0; o >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, o);
-	if (lane == 0 && rays) atomicAdd(ray_count, rays);
+	unsigned long long c[4] = {rays, c_nodes, c_leaves, c_iters};
+#pragma unroll
+	for (int k = 0; k < 4; ++k)
+		for (int o = 16; o > 0; o >>= 1) c[k] += __shfl_down_sync(0xffffffffu, c[k], o);
+	if (lane == 0) {
+		if (c[0]) atomicAdd(counts + TC_RAYS, c[0]);
+		if (c[1]) atomicAdd(counts + TC_NODES, c[1]);
+		if (c[2]) atomicAdd(counts + TC_LEAVES, c[2]);
+		if (c[3]) atomicAdd(counts + TC_PATCH_ITERS, c[3]);
+		if (c_warp) atomicAdd(counts + TC_WARP_STEPS, (unsigned long long)c_warp);
+		if (c_lanes) atomicAdd(counts + TC_LANE_STEPS, (unsigned long long)c_lanes);
+	}
 	if (err) atomicOr(status, err);
 }
 
@@ -549,13 +599,33 @@ __global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathS
 						for (int k = 0; k < 4; ++k) C.e[k] = fcol.e[k] * e.e[k];
 					}
 					for (int k = 0; k < 4; ++k) col.e[k] += C.e[k];
-					if (!W::BATCH && rp.grad) grad_add(rp, sgrad, ps, slot, vtx, C, lp, wl);
+					if (!W::BATCH && rp.grad) {
+						// the same contribution without its parameterised factors
+						const Spec e0 = rgb_to_spec(ecol, wl);
+						const Spec fx = sp(ps.fexcl[slot]);
+						Spec B;
+						if (!CAMERA && last_pdf != 0.0f) {
+							const float mis_inv_pdf = power_heuristic(last_pdf, lpdf) / last_pdf;
+							for (int k = 0; k < 4; ++k) B.e[k] = ((fx.e[k] * last_pdf) * e0.e[k]) * mis_inv_pdf;
+						} else {
+							for (int k = 0; k < 4; ++k) B.e[k] = fx.e[k] * e0.e[k];
+						}
+						grad_add(rp, sgrad, ps, slot, vtx, B, lp, wl);
+					}
 				} else if (closure != CLOSURE_LAMBERT) {
 					done = true;  // closures outside the supported set end the path
 				} else {
 					sh.pid = (rp.params && rec.shader >= 0) ? rp.shader_param[rec.shader] : -1;
 					if (!W::BATCH && rp.grad && vtx < PSY_ADJ_MAX_VERTS) {
-						const Spec a = sh.pid >= 0 ? albedo_spec(rp.params + sh.pid, wl) : Spec{};
+						Spec a = Spec{};
+						if (sh.pid >= 0) {
+							a = albedo_spec(rp.params + sh.pid, wl);
+						} else if (sh.pid < -1) {
+							const Spec up = rgb_to_spec(sh.col, wl);
+							const float q = rp.params[-2 - sh.pid];
+							for (int k = 0; k < 4; ++k) a.e[k] = up.e[k] * q;
+							ps.vdsc[slot * PSY_ADJ_MAX_VERTS + vtx] = f4(up);
+						}
 						ps.vpid[slot * PSY_ADJ_MAX_VERTS + vtx] = sh.pid;
 						ps.valb[slot * PSY_ADJ_MAX_VERTS + vtx] = f4(a);
 					}
@@ -609,6 +679,16 @@ __global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathS
 					Spec c;
 					for (int k = 0; k < 4; ++k) c.e[k] = (fcol.e[k] * lcol.e[k]) * fac.e[k];
 					contrib = f4(c);
+					if (!W::BATCH && rp.grad) {
+						// without the light's scale and the albedos of parameterised vertices
+						const Spec fx = sp(ps.fexcl[slot]);
+						const float cs = lambert_cos(sh.d, sray.d, sh.n);
+						const Spec f0 = sh.pid != -1 ? Spec{{cs, cs, cs, cs}} : fac;
+						Spec b;
+						for (int k = 0; k < 4; ++k)
+							b.e[k] = (fx.e[k] * (((q.spec.e[k] * mis_inv_pdf) * lc) / q.selection_pdf)) * f0.e[k];
+						ps.nee_base[slot] = f4(b);
+					}
 					stag = rid << 1;
 				} else {
 					err |= ERRF_NOLIGHT;
@@ -666,7 +746,8 @@ __global__ void __launch_bounds__(256) shade_shadow_kernel(W w, HaltonDev hd, Pa
 		if (wb.occl[i] == 0) {
 			const Spec c = sp(ps.lcol[slot]);
 			for (int k = 0; k < 4; ++k) col.e[k] += c.e[k];
-			if (!W::BATCH && rp.grad) grad_add(rp, sgrad, ps, slot, (int)(step >> 1) + 1, c, ps.nee_param[slot], wl);
+			if (!W::BATCH && rp.grad)
+				grad_add(rp, sgrad, ps, slot, (int)(step >> 1) + 1, sp(ps.nee_base[slot]), ps.nee_param[slot], wl);
 		}
 		step++;
 		if (step == rp.path_length * 2) {
@@ -701,6 +782,13 @@ __global__ void __launch_bounds__(256) shade_shadow_kernel(W w, HaltonDev hd, Pa
 		propagate_differentials(sh, &wr);
 		if (pdf < 0.00001f) pdf = 0.00001f;
 		for (int k = 0; k < 4; ++k) fcol.e[k] *= filter.e[k] / pdf;
+		if (!W::BATCH && rp.grad) {
+			// the path weight without the parameterised albedos
+			Spec fx = sp(ps.fexcl[slot]);
+			const float cs = lambert_cos(sh.d, out, sh.n);
+			for (int k = 0; k < 4; ++k) fx.e[k] *= (sh.pid != -1 ? cs : filter.e[k]) / pdf;
+			ps.fexcl[slot] = f4(fx);
+		}
 		store_ray(wb.ray[0], wb.cap, i, wr, rid << 1);
 		ps.dimstep[slot] = (dim & 0xffffu) | (step << 16);
 		ps.col[slot] = f4(col);
@@ -807,7 +895,8 @@ static void launch_wave(const W& w, uint32_t path_length, const HaltonDev& hd, c
 	c += 4;
 	for (uint32_t b = 0; b < path_length; ++b) {
 		tstart();
-		trace_wave_kernel<W, F, true><<<g.trace_o, block, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays + 1, status);
+		trace_wave_kernel<W, F, true><<<g.trace_o, block, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays + TC_COUNT,
+		                                                          status);
 		tstop();
 		shade_shadow_kernel<W><<<g.shadow, block, gsmem, st>>>(w, hd, ps, wb, q, n, c + 1);
 		*launches += 2;

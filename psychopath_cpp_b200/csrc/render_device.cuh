@@ -527,7 +527,7 @@ static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, floa
 		if (inst.xform_count > 0) {
 			const M44 X = seq_lerp_global(sc.xforms + (size_t)inst.xform * 16, inst.xform_count, q->time);
 			q->pos = pos_to(X, q->pos);
-			q->nor = normalized(nor_to(X, q->nor));
+			q->nor = normalized(nor_to(X, q->nor, sc.rcp));
 			q->xform = q->has_xform ? m44_mul(q->xform, X) : m44_mul(m44_identity(), X);
 			q->has_xform = true;
 		}
@@ -540,7 +540,7 @@ static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, floa
 			sphere_light_sample(sc, ob, q->pos, q->u, q->v, q->wavelength, q->time, &tl, &p, &q->spec);
 			// xform.dir_from: the reference inverts the accumulated transform,
 			// which is the identity when no instance carried one
-			if (q->has_xform) q->to_light = dir_from(q->xform, tl);
+			if (q->has_xform) q->to_light = dir_from(q->xform, tl, sc.rcp);
 			else q->to_light = tl * ident_inv;
 			q->selection_pdf *= (tot_prob * (float)as.light_count);
 			q->light_sample_pdf = p;

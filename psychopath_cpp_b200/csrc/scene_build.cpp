@@ -18,6 +18,8 @@
  */
 #include "scene_build.h"
 
+#include "host_cpu.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -83,16 +85,16 @@ std::vector<Box> transform_from(const std::vector<Box>& bbs_in, const M44* xs, i
 	std::vector<Box> bbs = bbs_in;
 	if (tcount == 0) {
 	} else if ((int)bbs.size() == tcount) {
-		for (size_t i = 0; i < bbs.size(); ++i) bbs[i] = box_inverse_transformed(bbs[i], xs[i]);
+		for (size_t i = 0; i < bbs.size(); ++i) bbs[i] = box_inverse_transformed(bbs[i], xs[i], host_rcp().table());
 	} else if ((int)bbs.size() > tcount) {
 		const float s = (float)(bbs.size() - 1);
 		for (size_t i = 0; i < bbs.size(); ++i)
-			bbs[i] = box_inverse_transformed(bbs[i], lerp_seq_m44((float)i / s, xs, tcount));
+			bbs[i] = box_inverse_transformed(bbs[i], lerp_seq_m44((float)i / s, xs, tcount), host_rcp().table());
 	} else {
 		const float s = (float)(tcount - 1);
 		std::vector<Box> t;
 		for (int i = 0; i < tcount; ++i)
-			t.push_back(box_inverse_transformed(lerp_seq_box((float)i / s, bbs), xs[i]));
+			t.push_back(box_inverse_transformed(lerp_seq_box((float)i / s, bbs), xs[i], host_rcp().table()));
 		bbs = std::move(t);
 	}
 	return bbs;
@@ -318,7 +320,8 @@ struct Builder {
 		const psy_instance_desc& id = ha.d->instances[i];
 		Box bb = lerp_seq_box(t, child_bounds_of(ha, i));
 		if (id.transform_count > 0)
-			bb = box_inverse_transformed(bb, lerp_seq_m44(t, ha.xforms.data() + id.transform_index, (int)id.transform_count));
+			bb = box_inverse_transformed(bb, lerp_seq_m44(t, ha.xforms.data() + id.transform_index, (int)id.transform_count),
+			                             host_rcp().table());
 		return bb;
 	}
 
@@ -750,7 +753,8 @@ struct Builder {
 					if (id.transform_count > 0)
 						l.bbox = box_inverse_transformed(lerp_seq_box(0.5f, sub.light_bounds),
 						                                 lerp_seq_m44(0.5f, ha.xforms.data() + id.transform_index,
-						                                              (int)id.transform_count));
+						                                              (int)id.transform_count),
+						                                 host_rcp().table());
 					else
 						l.bbox = lerp_seq_box(0.5f, sub.light_bounds);
 					l.center = box_center(l.bbox);

@@ -498,7 +498,7 @@ __device__ __forceinline__ bool patch_begin(PatchCursor<NV, TSC>& pc, const floa
 template <int NV, int TSC>
 __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<NV, TSC>& ps, const float* verts,
                                           const LocalRay& r, const RayWidth& rw, float* max_t, bool occl,
-                                          float dice_rate, float min_upoly, PatchHit* hit, int units) {
+                                          float dice_rate, float min_upoly, PatchHit* hit, int& units) {
 	constexpr int CP = PSY_PATCH_CP_STEP;
 	constexpr int NCP = PSY_PATCH_CP_COUNT;
 	Patch<NV>(&cur)[TSC] = pc.cur;
@@ -511,7 +511,8 @@ __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<N
 	auto& cps = ps.cps;
 	auto& cpuv = ps.cpuv;
 	while (true) {
-		if (units-- == 0) return false;
+		if (units == 0) return false;
+		--units;
 		// `cur` is a node whose box the ray hits; max_dim, h0, h1 are its test
 		// A NaN width (from NaN ray differentials: a grazing hit makes the
 		// next ray's origin differentials 0/0 in transfer_ray_origin_
@@ -627,7 +628,8 @@ __device__ bool patch_whole(const float* verts, float time, const LocalRay& r, c
 	PatchCursor<NV, TSC> pc;
 	PatchStore<NV, TSC> ps;
 	if (!patch_begin<NV, TSC>(pc, verts, time, r, *max_t)) return false;
-	patch_run<NV, TSC>(pc, ps, verts, r, rw, max_t, occl, dice_rate, min_upoly, hit, 0x7fffffff);
+	int units = 0x7fffffff;
+	patch_run<NV, TSC>(pc, ps, verts, r, rw, max_t, occl, dice_rate, min_upoly, hit, units);
 	return pc.found;
 }
 
@@ -1061,11 +1063,12 @@ __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState<F>& s)
 // The walk cut into pieces for kernels that group their lanes by the work
 // they do next: up to `nodes` inner-node visits, stopping at a leaf, which
 // is popped into s.leaf for leaf_visit.  Returns WALK_DONE when the ray is
-// finished, WALK_LEAF at a leaf, WALK_MORE when the visits ran out.
+// finished, WALK_LEAF at a leaf, WALK_MORE when the visits ran out; `nodes`
+// is left at the visits not used.
 enum : int { WALK_DONE = 0, WALK_LEAF = 1, WALK_MORE = 2 };
 
 template <unsigned F>
-__device__ __forceinline__ int walk_nodes(const DevScene& sc, TraceState<F>& s, int nodes) {
+__device__ __forceinline__ int walk_nodes(const DevScene& sc, TraceState<F>& s, int& nodes) {
 	while (true) {
 		leave_levels<F>(s);
 		if (s.nsp == 0) return WALK_DONE;
@@ -1075,7 +1078,8 @@ __device__ __forceinline__ int walk_nodes(const DevScene& sc, TraceState<F>& s, 
 			s.leaf = ref;
 			return WALK_LEAF;
 		}
-		if (nodes-- == 0) return WALK_MORE;
+		if (nodes == 0) return WALK_MORE;
+		--nodes;
 		--s.nsp;
 		if (!node_visit<F>(sc, s, ref)) return WALK_DONE;
 	}
@@ -1097,9 +1101,10 @@ __device__ __forceinline__ bool leaf_visit(const DevScene& sc, TraceState<F>& s)
 }
 
 // Carries the bisection in progress on for up to `units` iterations of its
-// loop.  Returns false when the ray is finished (an occlusion ray's hit).
+// loop (`units` is left at the iterations not used).  Returns false when
+// the ray is finished (an occlusion ray's hit).
 template <unsigned F>
-__device__ __forceinline__ bool patch_step(const DevScene& sc, TraceState<F>& s, int units) {
+__device__ __forceinline__ bool patch_step(const DevScene& sc, TraceState<F>& s, int& units) {
 	constexpr int TS = PatchBuf<F>::TS;
 	bool done = false, found = false;
 	float max_t = s.max_t;

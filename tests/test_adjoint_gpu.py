@@ -118,3 +118,111 @@ def test_emission_gradient_matches_reference(ctx, ref_available):
     mine = g[count - 8:]
     rel = np.abs(mine - ref_g) / np.abs(ref_g).max()
     assert np.all(rel < 5e-2), list(zip(mine, ref_g, rel))
+
+
+def _central_fd(r, p0, idx, target, h=1e-3):
+    fd = []
+    for i in idx:
+        pp = p0.clone()
+        pp[i] += h
+        lp = _loss(*r.forward(pp), target).item()
+        pm = p0.clone()
+        pm[i] -= h
+        lm = _loss(*r.forward(pm), target).item()
+        fd.append((lp - lm) / (2 * h))
+    return np.array(fd)
+
+
+def test_adjoint_at_zero_valued_parameters(ctx):
+    """A black albedo (all four weights 0) and a light scaled to 0 still get
+    their gradient: the derivative for one factor is the product of the
+    others, never a division by the factor."""
+    import torch
+    sc, r, p0, sp, op, count = _setup(ctx, res=(64, 64), spp=32)
+    rng = np.random.default_rng(7)
+    pt = p0 + torch.from_numpy(rng.normal(0.0, 0.1, count).astype(np.float32)).cuda()
+    tx, tc = r.forward(pt)
+    target = (tx.double().view(-1, 3) / tc.double().clamp(min=1).view(-1, 1)).detach()
+    p = p0.clone()
+    lights = np.arange(count - 8, count)
+    p[int(lights[0])] = 0.0                       # one light switched off
+    shaders, _, _, _ = api.flat_indices(sc)
+    # the four largest spheres get black albedos
+    big = sorted((n for n in sc.root.objects if n.startswith("sphere")),
+                 key=lambda n: -float(sc.root.objects[n].radius))[:4]
+    zeroed = []
+    for name in big:
+        w = int(sp[shaders[id(sc.root.shaders["mat" + name[6:]])]])
+        p[w:w + 4] = 0.0
+        zeroed += list(range(w, w + 4))
+    xyz, cnt = r.forward(p)
+    img = xyz.double().view(-1, 3) / cnt.double().view(-1, 1)
+    g = r.adjoint(p, (2.0 * (img - target) / cnt.double().view(-1, 1)).float().reshape(-1)).double().cpu().numpy()
+    idx = np.array([int(lights[0])] + zeroed[:8])
+    fd = _central_fd(r, p, idx, target)
+    assert np.all(np.abs(fd) > 0), fd
+    err = np.abs(g[idx] - fd) / np.maximum(np.abs(fd), 1e-3 * np.abs(fd).max())
+    assert np.all(err < 1e-2), list(zip(idx, g[idx], fd, err))
+
+
+def test_adjoint_config_size(ctx):
+    """The differentiable-render configuration: 256x256, 4 segments, 256
+    albedo weights + 8 emission scales, target from N(0, 0.1)-perturbed
+    parameters; the adjoint of the 4096-spp estimator against central
+    differences (h = 1e-3) of that estimator on 16 random parameters."""
+    import torch
+    res, spp = (256, 256), 4096
+    sc, r, p0, sp, op, count = _setup(ctx, res=res, spp=spp)
+    rng = np.random.default_rng(11)
+    pt = p0 + torch.from_numpy(rng.normal(0.0, 0.1, count).astype(np.float32)).cuda()
+    tx, tc = r.forward(pt)
+    target = (tx.double().view(-1, 3) / tc.double().clamp(min=1).view(-1, 1)).detach()
+    xyz, cnt = r.forward(p0)
+    img = xyz.double().view(-1, 3) / cnt.double().view(-1, 1)
+    dl = (2.0 * (img - target) / cnt.double().view(-1, 1)).float().reshape(-1)
+    g = r.adjoint(p0, dl).double().cpu().numpy()
+    idx = rng.choice(np.arange(count), 16, replace=False)
+    fd = _central_fd(r, p0, idx, target)
+    scale = np.abs(g).max()
+    err = np.abs(g[idx] - fd) / np.maximum(np.abs(fd), 1e-3 * scale)
+    assert np.all(err < 1e-2), list(zip(idx, g[idx], fd, err))
+
+
+def test_albedo_scale_gradient_matches_reference(ctx, ref_available):
+    """Albedo gradients pinned to the reference renderer: a parameter that
+    scales a shader's RGB albedo is the reference's albedo with its colour
+    scaled (the spectral upsampling is linear in the colour's magnitude, and
+    the reference's light selection does not read the albedo, so its paths
+    stay the same).  Central differences of reference renders with the
+    colour scaled by 1 +- h give the reference gradient of L = sum I^2."""
+    import torch
+    from oracle import psyref
+    res, spp, h = (48, 48), 256, 1e-2
+    sc = scenes.adjoint_scene(1, res=res, spp=spp)
+    ctx.upload(sc)
+    shaders, objects, ns, no = api.flat_indices(sc)
+    chosen = ["ground_mat"] + sorted((n for n in sc.root.objects if n.startswith("sphere")),
+                                      key=lambda n: -float(sc.root.objects[n].radius))[:4]
+    chosen = [c if c == "ground_mat" else "mat" + c[6:] for c in chosen]
+    ss = np.full(ns, -1, np.int32)
+    for k, name in enumerate(chosen):
+        ss[shaders[id(sc.root.shaders[name])]] = k
+    r = api.DiffRenderer(ctx, res[0], res[1], spp, np.full(ns, -1, np.int32), np.full(no, -1, np.int32), len(chosen),
+                         seed=1, path_length=4, shader_scale_param=ss)
+    p = torch.ones(len(chosen), dtype=torch.float32, device="cuda")
+    xyz, cnt = r.forward(p)
+    plain, _ = api.PathTraceIntegrator(ctx, res[0], res[1], spp, seed=1, path_length=4).integrate()
+    np.testing.assert_array_equal(plain.reshape(-1).view(np.uint32), xyz.cpu().numpy().view(np.uint32))
+    img = xyz.double().view(-1, 3) / cnt.double().view(-1, 1)
+    g = r.adjoint(p, (2.0 * img / cnt.double().view(-1, 1)).float().reshape(-1)).double().cpu().numpy()
+
+    def ref_loss(name, f):
+        s2 = scenes.adjoint_scene(1, res=res, spp=spp)
+        s2.root.shaders[name].color = s2.root.shaders[name].color * np.float32(f)
+        x, c, _, _ = psyref.RefScene(scene=s2).render(threads=0, spp=spp, path_length=4, seed=1)
+        im = x.reshape(-1, 3).astype(np.float64) / np.maximum(c.reshape(-1, 1), 1)
+        return (im ** 2).sum()
+
+    ref_g = np.array([(ref_loss(n, 1 + h) - ref_loss(n, 1 - h)) / (2 * h) for n in chosen])
+    rel = np.abs(g - ref_g) / np.abs(ref_g).max()
+    assert np.all(rel < 1e-2), list(zip(chosen, g, ref_g, rel))

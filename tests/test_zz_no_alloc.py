@@ -11,7 +11,7 @@ from tests import parity
 
 pytestmark = pytest.mark.gpu
 
-MAX_RAYS = 65536
+MAX_RAYS = _abi.PSY_NOALLOC_MAX_RAYS  # read from include/psy_b200.h
 ALL_FIELDS = tuple(api.HIT_FIELDS)
 
 
@@ -57,3 +57,26 @@ def test_noalloc_rejects_more_than_capacity(ctx):
         api.Tracer(ctx).trace_noalloc(rays)
     assert e.value.code == _abi.PSY_ERR_ARG
     assert "capacity" in str(e.value)
+
+
+def test_noalloc_hit_id_t_only_and_no_hits(ctx):
+    """Only hit, id and t requested (no geometry epilogue), and a call with
+    no hit arrays at all (hits = NULL), each against psy_trace_host."""
+    sc = scenes.many_light_scene(3, res=(32, 18), spp=1, n_patches=60, n_groups=20, n_lights=200)
+    ctx.upload(sc)
+    tr = api.Tracer(ctx)
+    rays = parity.random_rays(30000, (-6, -5, 0.0), (6, 5, 4), seed=31, occl_frac=0.4, width=0.01)
+    fields = ("hit", "id", "t")
+    _same(tr.trace(rays, fields=fields), tr.trace_noalloc(rays, fields=fields))
+    assert tr.trace_noalloc(rays, fields=None) == {}
+    # the array still serves a full call after the call without hits
+    _same(tr.trace(rays, fields=ALL_FIELDS), tr.trace_noalloc(rays, fields=ALL_FIELDS))
+
+
+def test_noalloc_zero_rays_is_a_warm_up(ctx):
+    """n = 0 only makes the fixed array resident: it succeeds and returns
+    empty results."""
+    rays = parity.random_rays(1, (0, 0, 0), (1, 1, 1), seed=1)
+    empty = {k: v[:0] for k, v in rays.items()}
+    out = api.Tracer(ctx).trace_noalloc(empty, fields=("hit", "id", "t"))
+    assert all(v.shape[0] == 0 for v in out.values())
