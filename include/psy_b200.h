@@ -318,6 +318,19 @@ int psy_render(psy_ctx* ctx, const psy_render_desc* desc, float* xyz, uint32_t* 
                void* stream);
 
 /*
+ * Film output (Film::scanline_image_8bbc, film/film.hpp:173-225): the film
+ * psy_render accumulates (device xyz sums, width*height*3, and counts,
+ * width*height) to 8-bit sRGB scanlines (device rgb, width*height*3):
+ * mean XYZ -> whitepoint-E sRGB, clamped, sRGB curve, x255, dither,
+ * clamp, truncate; pixels without samples show the reference's grey
+ * checkerboard.  The reference dithers with a clock-seeded RNG; here the
+ * dither is a hash of (seed, pixel, channel) in [-0.5, 0.5) when `dithered`
+ * is non-zero, else none.  Stream-ordered on `stream`.
+ */
+int psy_film_srgb8(psy_ctx* ctx, const float* xyz, const uint32_t* counts, uint32_t width, uint32_t height,
+                   int dithered, uint32_t seed, uint8_t* rgb, void* stream);
+
+/*
  * Optional timing of the traversal kernels, for roofline reports (no
  * counterpart in the reference).  While enabled, psy_render records CUDA
  * events on its stream around every traversal launch (the event pool starts

@@ -15,20 +15,25 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libpsyref.so")
+# The same reference build with tracer/tracer.cpp replaced by the reference-side
+# bridge (oracle/ref/psy_bridge.cpp): its Tracer::trace calls libpsy_b200.
+BRIDGED_LIB_PATH = os.path.join(HERE, "_ref", "libpsyref_bridged.so")
 
-_lib = None
+_libs = {}
 
 
-def available() -> bool:
-    return os.path.exists(LIB_PATH)
+def available(bridged: bool = False) -> bool:
+    return os.path.exists(BRIDGED_LIB_PATH if bridged else LIB_PATH)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
-            raise RuntimeError("oracle/_ref/libpsyref.so is not built (make -C oracle ref)")
-        L = C.CDLL(LIB_PATH)
+def lib(bridged: bool = False):
+    """The reference build (or its bridged form, whose tracer runs on the
+    B200 library at `psy_lib`, set with set_bridge_library first)."""
+    if bridged not in _libs:
+        path = BRIDGED_LIB_PATH if bridged else LIB_PATH
+        if not os.path.exists(path):
+            raise RuntimeError("%s is not built (make -C oracle %s)" % (path, "bridged" if bridged else "ref"))
+        L = C.CDLL(path)
         vp, sz, fp, u64p, u32p, u8p, u16p, dp = (C.c_void_p, C.c_size_t, C.POINTER(C.c_float),
                                                   C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
                                                   C.POINTER(C.c_uint8), C.POINTER(C.c_uint16),
@@ -47,6 +52,7 @@ def lib():
         L.psyref_halton.argtypes = [sz, u32p, u32p, fp]
         L.psyref_sampler.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, fp, u32p]
         L.psyref_eval.argtypes = [C.c_int, sz, fp, C.c_int, fp, C.c_int]
+        L.psyref_film_srgb8.argtypes = [fp, u32p, C.c_int, C.c_int, u8p]
         L.psyref_assembly_count.restype = C.c_int
         L.psyref_assembly_count.argtypes = [vp]
         L.psyref_bvh4_node_count.restype = sz
@@ -58,8 +64,15 @@ def lib():
         L.psyref_lighttree_bounds_count.argtypes = [vp, C.c_int]
         L.psyref_lighttree_nodes.argtypes = [vp, C.c_int, u64p, fp, fp]
         L.psyref_lighttree_totals.argtypes = [vp, C.c_int, u64p, fp]
-        _lib = L
-    return _lib
+        if bridged:
+            L.psy_bridge_set_library.argtypes = [C.c_char_p]
+        _libs[bridged] = L
+    return _libs[bridged]
+
+
+def set_bridge_library(psy_lib_path: str) -> None:
+    """Which libpsy_b200.so the bridged reference traces with."""
+    lib(True).psy_bridge_set_library(psy_lib_path.encode())
 
 
 def _p(a, t):
@@ -82,8 +95,9 @@ def rays_to_flat(rays: dict) -> np.ndarray:
 class RefScene:
     """A parsed and finalized reference Scene."""
 
-    def __init__(self, psy_path: Optional[str] = None, scene=None):
-        L = lib()
+    def __init__(self, psy_path: Optional[str] = None, scene=None, bridged: bool = False):
+        self.bridged = bridged
+        L = self.L = lib(bridged)
         tmp = None
         if psy_path is None:
             fd, tmp = tempfile.mkstemp(suffix=".psy")
@@ -104,7 +118,7 @@ class RefScene:
 
     def close(self):
         if self.h:
-            lib().psyref_free(self.h)
+            self.L.psyref_free(self.h)
             self.h = None
 
     def __del__(self):
@@ -114,7 +128,7 @@ class RefScene:
             pass
 
     def _use(self):
-        lib().psyref_set_dice_rate(self.dice_rate)
+        self.L.psyref_set_dice_rate(self.dice_rate)
 
     def render(self, threads: int = 0, spp: int = 0, path_length: int = 4, seed: int = -1):
         """Returns (xyz sums [h,w,3], counts [h,w], rays_shot, seconds)."""
@@ -124,7 +138,7 @@ class RefScene:
         cnt = np.zeros((self.res_y, self.res_x), np.uint32)
         rays = C.c_uint64()
         secs = C.c_double()
-        lib().psyref_render(self.h, threads, spp, path_length, seed, _p(xyz, C.c_float), _p(cnt, C.c_uint32),
+        self.L.psyref_render(self.h, threads, spp, path_length, seed, _p(xyz, C.c_float), _p(cnt, C.c_uint32),
                             C.byref(rays), C.byref(secs))
         return xyz, cnt, rays.value, secs.value
 
@@ -137,7 +151,7 @@ class RefScene:
         hit = np.zeros(n, np.uint8)
         ids = np.zeros(n, np.uint64)
         out = np.zeros((n, 48), np.float32) if full else None
-        secs = lib().psyref_trace(self.h, n, _p(flat, C.c_float), _p(types, C.c_uint16), threads or os.cpu_count(),
+        secs = self.L.psyref_trace(self.h, n, _p(flat, C.c_float), _p(types, C.c_uint16), threads or os.cpu_count(),
                                   chunk, _p(hit, C.c_uint8), _p(ids, C.c_uint64), _p(out, C.c_float))
         res = {"hit": hit, "id": ids, "seconds": secs}
         if full:
@@ -150,41 +164,41 @@ class RefScene:
         q = np.ascontiguousarray(q, np.float32).reshape(-1, 15)
         out = np.zeros((q.shape[0], 14), np.float32)
         ids = np.zeros(q.shape[0], np.uint64)
-        lib().psyref_light_sample(self.h, q.shape[0], _p(q, C.c_float), _p(out, C.c_float), _p(ids, C.c_uint64))
+        self.L.psyref_light_sample(self.h, q.shape[0], _p(q, C.c_float), _p(out, C.c_float), _p(ids, C.c_uint64))
         return out, ids
 
     def camera_rays(self, args: np.ndarray) -> np.ndarray:
         args = np.ascontiguousarray(args, np.float32).reshape(-1, 7)
         out = np.zeros((args.shape[0], 19), np.float32)
-        lib().psyref_camera_ray(self.h, args.shape[0], _p(args, C.c_float), _p(out, C.c_float))
+        self.L.psyref_camera_ray(self.h, args.shape[0], _p(args, C.c_float), _p(out, C.c_float))
         return out
 
     def assembly_count(self) -> int:
-        return lib().psyref_assembly_count(self.h)
+        return self.L.psyref_assembly_count(self.h)
 
     def bvh4_nodes(self, assembly: int = 0):
-        n = lib().psyref_bvh4_node_count(self.h, assembly)
+        n = self.L.psyref_bvh4_node_count(self.h, assembly)
         b = np.zeros((n, 24), np.float32)
         ch = np.zeros((n, 3), np.uint64)
         ts = np.zeros(n, np.uint32)
         di = np.zeros(n, np.uint64)
         if n:
-            lib().psyref_bvh4_nodes(self.h, assembly, _p(b, C.c_float), _p(ch, C.c_uint64), _p(ts, C.c_uint32),
+            self.L.psyref_bvh4_nodes(self.h, assembly, _p(b, C.c_float), _p(ch, C.c_uint64), _p(ts, C.c_uint32),
                                     _p(di, C.c_uint64))
         return {"bounds": b, "child": ch, "ts": ts, "data_index": di}
 
     def light_tree(self, assembly: int = 0):
-        n = lib().psyref_lighttree_node_count(self.h, assembly)
-        nb = lib().psyref_lighttree_bounds_count(self.h, assembly)
+        n = self.L.psyref_lighttree_node_count(self.h, assembly)
+        nb = self.L.psyref_lighttree_bounds_count(self.h, assembly)
         meta = np.zeros((n, 6), np.uint64)
         en = np.zeros(n, np.float32)
         bb = np.zeros((max(nb, 1), 6), np.float32)
         if n:
-            lib().psyref_lighttree_nodes(self.h, assembly, _p(meta, C.c_uint64), _p(en, C.c_float),
+            self.L.psyref_lighttree_nodes(self.h, assembly, _p(meta, C.c_uint64), _p(en, C.c_float),
                                          _p(bb, C.c_float))
         cnt = C.c_uint64()
         tot = C.c_float()
-        lib().psyref_lighttree_totals(self.h, assembly, C.byref(cnt), C.byref(tot))
+        self.L.psyref_lighttree_totals(self.h, assembly, C.byref(cnt), C.byref(tot))
         return {"meta": meta, "energy": en, "bounds": bb[:nb], "light_count": cnt.value, "total_energy": tot.value}
 
 
@@ -208,4 +222,15 @@ def eval_fn(fn: int, inputs: np.ndarray, out_stride: int) -> np.ndarray:
     n, k = inputs.shape
     out = np.zeros((n, out_stride), np.float32)
     lib().psyref_eval(fn, n, _p(inputs, C.c_float), k, _p(out, C.c_float), out_stride)
+    return out
+
+
+def film_srgb8(xyz: np.ndarray, counts: np.ndarray) -> np.ndarray:
+    """Film::scanline_image_8bbc of a film with these sums (h, w, 3) and
+    counts (h, w), with the reference film's own (clock-seeded) dither."""
+    h, w = counts.shape
+    xyz = np.ascontiguousarray(xyz, np.float32)
+    counts = np.ascontiguousarray(counts, np.uint32)
+    out = np.zeros((h, w, 3), np.uint8)
+    lib().psyref_film_srgb8(_p(xyz, C.c_float), _p(counts, C.c_uint32), w, h, _p(out, C.c_uint8))
     return out

@@ -217,6 +217,27 @@ int psyref_render(void* h, int threads, int spp, int path_length, int seed,
 }
 
 /*
+ * Film::scanline_image_8bbc (film/film.hpp:173-225) of a film holding the
+ * given per-pixel XYZ sums and sample counts (w*h*3 floats, w*h counts,
+ * scanline order), with the film's own dither; out: w*h*3 bytes.
+ */
+void psyref_film_srgb8(const float* xyz, const uint32_t* counts, int w, int ht, uint8_t* out) {
+	Film film(w, ht, -1.0, -((static_cast<float>(ht)) / w), 1.0, ((static_cast<float>(ht)) / w));
+	for (int y = 0; y < ht; ++y) {
+		for (int x = 0; x < w; ++x) {
+			const size_t i = (size_t)y * w + x;
+			film.pixels(x, y) = Color_XYZ();
+			film.pixels(x, y).x = xyz[3 * i];
+			film.pixels(x, y).y = xyz[3 * i + 1];
+			film.pixels(x, y).z = xyz[3 * i + 2];
+			film.accum(x, y) = counts[i];
+		}
+	}
+	const std::vector<uint8_t> im = film.scanline_image_8bbc();
+	std::copy(im.begin(), im.end(), out);
+}
+
+/*
  * Traces n world rays through Tracer::trace, in chunks of `chunk` rays (the
  * reference's own streams are about 65,536 long), on `threads` threads with
  * one Tracer each.
@@ -366,6 +387,7 @@ void psyref_sampler(uint32_t x, uint32_t y, uint32_t s, uint32_t seed, int count
  *   6 wavelength_n(hero, i) for i=0..3         -> 4        in: hero
  *   7 zup_to_vec(from, toz)                    -> 3        in: from(3) toz(3)
  *   8 Matrix44::inverse                        -> 16       in: m(16)
+ *   9 XYZ_to_sRGB_E(xyz)                       -> 3        in: x y z
  * `in_stride`/`out_stride` are the per-item float counts.
  */
 void psyref_eval(int fn, size_t n, const float* in, int in_stride, float* out, int out_stride) {
@@ -411,6 +433,12 @@ void psyref_eval(int fn, size_t n, const float* in, int in_stride, float* out, i
 				Matrix44 inv = m.inverse();
 				for (int r = 0; r < 4; ++r)
 					for (int c = 0; c < 4; ++c) o[r * 4 + c] = inv[r][c];
+				break;
+			}
+			case 9: {
+				Color_XYZ c;
+				c.x = a[0]; c.y = a[1]; c.z = a[2];
+				std::tie(o[0], o[1], o[2]) = XYZ_to_sRGB_E(c);
 				break;
 			}
 			default: break;

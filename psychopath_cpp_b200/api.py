@@ -385,6 +385,55 @@ class PathTraceIntegrator:
         return xyz.cpu().numpy().reshape(h, w, 3), cnt.cpu().numpy().reshape(h, w).astype(np.uint32)
 
 
+class Film:
+    """The film of a render (the reference's Film, film/film.hpp): per-pixel
+    XYZ sums and sample counts as psy_render accumulates them, its 8-bit
+    sRGB image (psy_film_srgb8, Film::scanline_image_8bbc) and the image
+    files the reference writes with OpenImageIO (renderer/renderer.cpp:24-42;
+    OpenImageIO is absent, so PPM for the 8-bit image and PFM for the mean
+    XYZ are written here)."""
+
+    def __init__(self, ctx: Context, xyz, counts, width: int, height: int):
+        self.ctx, self.xyz, self.counts, self.width, self.height = ctx, xyz, counts, width, height
+
+    def srgb8(self, dither_seed: Optional[int] = 0, stream=None):
+        """(h, w, 3) uint8 device tensor; dither_seed None = no dither."""
+        torch = _torch()
+        out = torch.empty(self.height * self.width * 3, dtype=torch.uint8, device=self.xyz.device)
+        self.ctx.check(self.ctx.L.psy_film_srgb8(self.ctx.h, C.c_void_p(self.xyz.data_ptr()),
+                                                 C.c_void_p(self.counts.data_ptr()), self.width, self.height,
+                                                 0 if dither_seed is None else 1, int(dither_seed or 0) & 0xffffffff,
+                                                 C.c_void_p(out.data_ptr()), stream))
+        return out.view(self.height, self.width, 3)
+
+    def write_ppm(self, path: str, dither_seed: Optional[int] = 0) -> None:
+        """Binary PPM (P6) of the 8-bit sRGB image, scanlines top to bottom."""
+        rgb = self.srgb8(dither_seed).cpu().numpy()
+        with open(path, "wb") as f:
+            f.write(b"P6\n%d %d\n255\n" % (self.width, self.height))
+            f.write(np.ascontiguousarray(rgb).tobytes())
+
+    def write_pfm(self, path: str) -> None:
+        """PFM (little-endian, three channels) of the mean XYZ per pixel
+        (0 where no sample landed), rows bottom to top as PFM stores them."""
+        x = self.xyz.detach().cpu().numpy().reshape(self.height, self.width, 3).astype(np.float32)
+        c = self.counts.detach().cpu().numpy().reshape(self.height, self.width, 1).astype(np.float32)
+        mean = np.where(c > 0, x / np.maximum(c, 1), 0.0).astype("<f4")
+        with open(path, "wb") as f:
+            f.write(b"PF\n%d %d\n-1.0\n" % (self.width, self.height))
+            f.write(np.ascontiguousarray(mean[::-1]).tobytes())
+
+
+def read_ppm(path: str) -> np.ndarray:
+    """Reads a binary PPM (P6, maxval 255) written by Film.write_ppm."""
+    with open(path, "rb") as f:
+        data = f.read()
+    parts = data.split(b"\n", 3)
+    assert parts[0] == b"P6" and parts[2] == b"255"
+    w, h = (int(v) for v in parts[1].split())
+    return np.frombuffer(parts[3], np.uint8).reshape(h, w, 3)
+
+
 class BatchRenderer:
     """Many renders of different scenes in one stream of waves
     (psy_render_batch).  `entries` are dicts with `scene` (a Context holding

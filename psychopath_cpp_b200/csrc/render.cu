@@ -496,7 +496,13 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 		++c_warp;
 		c_lanes += __popc(run == 1 ? nmask : run == 2 ? lmask : pmask);
 		bool live = true;
-		if (kind == run) {
+		if (run == 3) {
+			// bisections: every lane takes part in the warp-cooperative step,
+			// the lanes without one only in its votes
+			int left = PSY_PATCH_UNITS;
+			live = patch_step_warp<F>(w.scene(rid), st, kind == 3, left);
+			if (kind == 3) c_iters += PSY_PATCH_UNITS - left;
+		} else if (kind == run) {
 			const DevScene& sc = w.scene(rid);
 			if (run == 1) {
 				int left = PSY_WALK_NODES;
@@ -504,14 +510,10 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 				c_nodes += PSY_WALK_NODES - left;
 				live = r != WALK_DONE;
 				at_leaf = r == WALK_LEAF;
-			} else if (run == 2) {
+			} else {
 				at_leaf = false;
 				++c_leaves;
 				live = leaf_visit<F>(sc, st);
-			} else {
-				int left = PSY_PATCH_UNITS;
-				live = patch_step<F>(sc, st, left);
-				c_iters += PSY_PATCH_UNITS - left;
 			}
 		}
 		if (!live) {

@@ -63,3 +63,22 @@ def test_parser_handles_comments_escapes_and_defaults():
 def test_malformed_files_raise(bad):
     with pytest.raises(S.PsyParseError):
         S.parse_psy(bad)
+
+
+def test_film_pfm_round_trip(tmp_path):
+    """Film.write_pfm: mean XYZ per pixel, rows bottom to top, little-endian."""
+    import torch
+    from psychopath_cpp_b200 import api
+    rng = np.random.default_rng(2)
+    w, h = 7, 5
+    xyz = rng.uniform(0, 3, (h, w, 3)).astype(np.float32)
+    cnt = rng.integers(0, 4, (h, w)).astype(np.int32)
+    film = api.Film(None, torch.from_numpy(xyz.reshape(-1)), torch.from_numpy(cnt.reshape(-1)), w, h)
+    path = str(tmp_path / "f.pfm")
+    film.write_pfm(path)
+    data = open(path, "rb").read()
+    header, rest = data.split(b"\n", 3)[:3], data.split(b"\n", 3)[3]
+    assert header == [b"PF", b"7 5", b"-1.0"]
+    img = np.frombuffer(rest, "<f4").reshape(h, w, 3)[::-1]
+    expect = np.where(cnt[..., None] > 0, xyz / np.maximum(cnt[..., None], 1), 0)
+    np.testing.assert_allclose(img, expect, rtol=1e-6)
