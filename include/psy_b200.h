@@ -135,6 +135,22 @@ typedef struct psy_scene_desc {
  */
 int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* scene);
 
+/*
+ * psy_scene_upload with options (no counterpart in the reference, whose
+ * builds run on the host at Assembly::finalize).  PSY_UPLOAD_GPU_BVH: the
+ * root assembly's traversal BVH4 is built on the device (a linear BVH over
+ * the instances' boxes: Morton-sorted centres, binary radix tree, bottom-up
+ * boxes, packed four-wide as BVH4::build packs, accel/bvh4.cpp:17-159),
+ * when no root instance has motion (otherwise the host builds it as
+ * psy_scene_upload does).  Hits are those of psy_scene_upload (exact ties
+ * aside): only the tree that orders the candidates differs.  The light
+ * tree and the nested assemblies' trees are built on the host either way
+ * (the light tree's structure decides light selection, so it stays the
+ * reference's).
+ */
+#define PSY_UPLOAD_GPU_BVH 1u
+int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* scene, uint32_t flags);
+
 /* Summary of the uploaded scene (for tests and tooling). */
 typedef struct psy_scene_stats {
 	uint32_t assemblies, instances, objects, bvh4_nodes, light_nodes, lights;

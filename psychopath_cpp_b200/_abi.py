@@ -40,6 +40,7 @@ def header_define(name: str) -> int:
 
 
 PSY_NOALLOC_MAX_RAYS = header_define("PSY_NOALLOC_MAX_RAYS")
+PSY_UPLOAD_GPU_BVH = header_define("PSY_UPLOAD_GPU_BVH")
 
 fp = C.POINTER(C.c_float)
 u8p = C.POINTER(C.c_uint8)
@@ -141,6 +142,7 @@ class TraceCounters(C.Structure):
 
 # every symbol declared in include/psy_b200.h
 EXPORTED = ["psy_ctx_create", "psy_ctx_destroy", "psy_last_error", "psy_version", "psy_scene_upload",
+            "psy_scene_upload_ex",
             "psy_scene_stats_get", "psy_build_bvh4", "psy_build_light_tree", "psy_trace", "psy_trace_host", "psy_sync",
             "psy_trace_host_noalloc", "psy_render_batch", "psy_batch_autotune", "psy_render_diff",
             "psy_render_adjoint", "psy_profile_enable", "psy_profile_read", "psy_profile_counters",
@@ -163,6 +165,8 @@ def load():
     L.psy_last_error.restype = C.c_char_p
     L.psy_version.restype = C.c_char_p
     L.psy_scene_upload.argtypes = [C.c_void_p, C.POINTER(SceneDesc)]
+    if hasattr(L, "psy_scene_upload_ex"):
+        L.psy_scene_upload_ex.argtypes = [C.c_void_p, C.POINTER(SceneDesc), C.c_uint32]
     L.psy_scene_stats_get.argtypes = [C.c_void_p, C.POINTER(SceneStats)]
     L.psy_build_bvh4.argtypes = [C.POINTER(SceneDesc), C.c_uint32, u64p, fp, u64p, u32p, u64p]
     L.psy_build_light_tree.argtypes = [C.POINTER(SceneDesc), C.c_uint32, u64p, u64p, u64p, fp, fp, u64p, fp]

@@ -170,9 +170,14 @@ class Context:
         if rc != 0:
             raise _abi.PsyError(rc, self.L.psy_last_error(self.h).decode())
 
-    def upload(self, scene: Scene) -> None:
+    def upload(self, scene: Scene, gpu_bvh: bool = False) -> None:
+        """psy_scene_upload; gpu_bvh builds the root's traversal BVH4 on the
+        device (psy_scene_upload_ex with PSY_UPLOAD_GPU_BVH)."""
         desc, keep = flatten(scene)
-        self.check(self.L.psy_scene_upload(self.h, C.byref(desc)))
+        if gpu_bvh:
+            self.check(self.L.psy_scene_upload_ex(self.h, C.byref(desc), _abi.PSY_UPLOAD_GPU_BVH))
+        else:
+            self.check(self.L.psy_scene_upload(self.h, C.byref(desc)))
         del keep
         self.scene = scene
 

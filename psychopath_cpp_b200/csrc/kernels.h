@@ -158,6 +158,13 @@ cudaError_t launch_light_sample(const DevScene& sc, const LightQuerySoADev& q, c
 cudaError_t launch_trace(const DevScene& sc, const RaySoA& rays, const HitSoA& hits, uint32_t n, unsigned* status,
                          cudaStream_t stream);
 
+// Device build of a BVH4 over n leaf boxes (host, 6 floats each: lo xyz,
+// hi xyz; leaf k is local instance k).  The nodes go to d_nodes[0..] (room
+// for n - 1), numbered from node_base in their child references; *root_ref
+// and *node_count describe the result.  Synchronous on `st` (bvh_gpu.cu).
+cudaError_t build_bvh4_gpu(const float* h_boxes, int n, int node_base, DevNode* d_nodes, int* root_ref,
+                           int* node_count, cudaStream_t st);
+
 }  // namespace psy
 
 #endif

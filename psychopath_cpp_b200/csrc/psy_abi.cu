@@ -560,12 +560,15 @@ const char* psy_last_error(const psy_ctx* ctx) {
 	return ctx->last_error.c_str();
 }
 
-int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* desc) {
+int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* desc) { return psy_scene_upload_ex(ctx, desc, 0u); }
+
+int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags) {
 	if (!ctx) return PSY_ERR_ARG;
+	if (flags & ~PSY_UPLOAD_GPU_BVH) return ctx_fail(ctx, PSY_ERR_ARG, "psy_scene_upload_ex: unknown flags %#x", flags);
 	cudaSetDevice(ctx->device);
 	std::unique_ptr<BuiltScene> b(new BuiltScene());
 	std::string err;
-	int rc = build_scene(desc, b.get(), &err);
+	int rc = build_scene(desc, b.get(), &err, (flags & PSY_UPLOAD_GPU_BVH) != 0);
 	if (rc != PSY_OK) return ctx_fail(ctx, rc, "scene: %s", err.c_str());
 	ctx->free_scene();
 	DevScene& d = ctx->dev;
@@ -573,10 +576,33 @@ int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* desc) {
 #define UP(field, vec)                                                                        \
 	if ((rc = ctx->upload(vec.data(), vec.size() * sizeof(vec[0]), &p)) != PSY_OK) return rc; \
 	d.field = static_cast<decltype(d.field)>(p);
+	ctx->gpu_bvh_nodes = -1;
+	if (b->gpu_root_pending) {
+		// the host-built nodes, then room for the root's device-built ones
+		const int n = (int)(b->gpu_leaf_boxes.size() / 6);
+		const size_t host_nodes = b->nodes.size();
+		const size_t cap = host_nodes + (size_t)(n > 1 ? n - 1 : 0);
+		void* np = nullptr;
+		if ((rc = ctx_cuda(ctx, cudaMalloc(&np, (cap ? cap : 1) * sizeof(DevNode)), "cudaMalloc(nodes)"))) return rc;
+		ctx->scene_allocs.push_back(np);
+		ctx->device_bytes += cap * sizeof(DevNode);
+		if (host_nodes && (rc = ctx_cuda(ctx, cudaMemcpy(np, b->nodes.data(), host_nodes * sizeof(DevNode),
+		                                                 cudaMemcpyHostToDevice), "cudaMemcpy(nodes)")))
+			return rc;
+		int root = REF_EMPTY, count = 0;
+		if ((rc = ctx_cuda(ctx, build_bvh4_gpu(b->gpu_leaf_boxes.data(), n, (int)host_nodes,
+		                                       static_cast<DevNode*>(np) + host_nodes, &root, &count, nullptr),
+		                   "psy_scene_upload_ex: device BVH build")))
+			return rc;
+		b->assemblies[0].root = root;
+		ctx->gpu_bvh_nodes = count;
+		d.nodes = static_cast<const DevNode*>(np);
+	} else {
+		UP(nodes, b->nodes);
+	}
 	UP(assemblies, b->assemblies);
 	UP(instances, b->instances);
 	UP(objects, b->objects);
-	UP(nodes, b->nodes);
 	UP(node_extra, b->node_extra);
 	UP(xforms, b->xforms);
 	UP(fpool, b->fpool);
@@ -614,7 +640,7 @@ int psy_scene_stats_get(const psy_ctx* ctx, psy_scene_stats* out) {
 	out->assemblies = (uint32_t)ctx->host->assemblies.size();
 	out->instances = (uint32_t)ctx->host->instances.size();
 	out->objects = (uint32_t)ctx->host->objects.size();
-	out->bvh4_nodes = (uint32_t)ctx->host->nodes.size();
+	out->bvh4_nodes = (uint32_t)ctx->host->nodes.size() + (uint32_t)(ctx->gpu_bvh_nodes > 0 ? ctx->gpu_bvh_nodes : 0);
 	out->light_nodes = (uint32_t)ctx->host->light_nodes.size();
 	out->lights = ctx->host->total_lights;
 	out->device_bytes = ctx->device_bytes;

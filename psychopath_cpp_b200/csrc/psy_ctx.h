@@ -53,6 +53,8 @@ struct psy_ctx {
 	psy::LaunchTimer timer{};
 	// traversal counters of the last psy_render* call (its scratch buffer)
 	const unsigned long long* last_counts = nullptr;
+	// BVH4 nodes the last upload built on the device (-1: built on the host)
+	int gpu_bvh_nodes = -1;
 
 	~psy_ctx();
 	void free_scene();

@@ -152,6 +152,7 @@ struct Builder {
 	const psy_scene_desc* desc;
 	BuiltScene* out;
 	std::string* err;
+	bool gpu_root_bvh = false;
 	std::vector<HObject> objs;
 	std::vector<HAssembly> asms;
 	std::vector<int> asm_inst_base;
@@ -804,10 +805,34 @@ struct Builder {
 	}
 
 	// ---------------------------------------------------------------
+	// The root's leaf boxes for the device build, when every root instance
+	// has a single bounding box; false otherwise.
+	bool root_leaves_for_gpu(HAssembly& ha) {
+		std::vector<float> boxes;
+		for (uint32_t i = 0; i < ha.d->instance_count; ++i) {
+			const std::vector<Box> bbs = instance_bounds(ha, i);
+			if (bbs.size() != 1) return false;
+			const Box& b = bbs[0];
+			boxes.insert(boxes.end(), {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z});
+		}
+		out->gpu_leaf_boxes.swap(boxes);
+		out->gpu_root_pending = true;
+		out->assemblies[0].root = REF_EMPTY;
+		return true;
+	}
+
 	int finalize(int a, int depth) {
 		HAssembly& ha = asms[a];
 		int maxd = depth;
 		for (int c : ha.children) maxd = std::max(maxd, finalize(c, depth + 1));
+		// the root is never instanced, so its reference-form tree (which gives
+		// an assembly its bounds) is not needed when the device builds its
+		// traversal tree
+		if (a == 0 && gpu_root_bvh && root_leaves_for_gpu(ha)) {
+			build_light_tree(ha, a);
+			ha.finalized = true;
+			return maxd;
+		}
 		build_bvh4(ha, a, false);
 		build_bvh4(ha, a, true);
 		build_light_tree(ha, a);
@@ -898,11 +923,12 @@ struct Builder {
 
 }  // namespace
 
-int build_scene(const psy_scene_desc* desc, BuiltScene* out, std::string* err) {
+int build_scene(const psy_scene_desc* desc, BuiltScene* out, std::string* err, bool gpu_root_bvh) {
 	Builder b;
 	b.desc = desc;
 	b.out = out;
 	b.err = err;
+	b.gpu_root_bvh = gpu_root_bvh;
 	return b.run() ? PSY_OK : PSY_ERR_ARG;
 }
 

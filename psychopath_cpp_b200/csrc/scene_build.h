@@ -41,11 +41,19 @@ struct BuiltScene {
 	unsigned features = 0;  // FEAT_* present
 	uint32_t total_lights = 0;
 	std::vector<RefBVH4> ref_bvh4;    // per assembly
+	// With gpu_root_bvh requested and a root assembly whose instances all
+	// have one bounding box (no motion), the root's traversal BVH4 is left
+	// to the device build: its leaf boxes are here, in instance order, and
+	// assemblies[0].root stays REF_EMPTY until that build sets it.
+	bool gpu_root_pending = false;
+	std::vector<float> gpu_leaf_boxes;  // per root instance: lo xyz, hi xyz
 };
 
 // Validates the description and builds every assembly (children first).
-// Returns PSY_OK or PSY_ERR_ARG with *err set.
-int build_scene(const psy_scene_desc* desc, BuiltScene* out, std::string* err);
+// gpu_root_bvh: leave the root assembly's traversal tree to the device
+// build when it has no motion (see gpu_root_pending).  Returns PSY_OK or
+// PSY_ERR_ARG with *err set.
+int build_scene(const psy_scene_desc* desc, BuiltScene* out, std::string* err, bool gpu_root_bvh = false);
 
 }  // namespace psy
 

@@ -188,3 +188,38 @@ def test_nan_differentials_end_at_min_upoly(ctx, ref_available):
     np.testing.assert_array_equal(ref["t"], mine_zero["t"])
     for k in ("hit", "id", "t", "uv"):
         np.testing.assert_array_equal(mine_zero[k], mine_nan[k])
+
+
+@pytest.mark.parametrize("kind", ["batch", "heightfield"])
+def test_device_built_bvh_gives_the_same_hits(ctx, ref_available, kind):
+    """psy_scene_upload_ex(PSY_UPLOAD_GPU_BVH): the root's traversal BVH4
+    built on the device (linear BVH) instead of the host's surface-area
+    tree.  Only the order candidates are met changes: the hits agree with the
+    reference's and with the host-built tree's."""
+    from oracle import psyref
+    if kind == "batch":
+        sc = scenes.batch_scene(10, (64, 48), 4, 20000, 20)
+        rays = parity.random_rays(60000, (-7, -7, -0.5), (7, 7, 4), seed=41, occl_frac=0.3, width=0.002)
+    else:
+        sc = scenes.heightfield_scene(64, seed=5)
+        rays = scenes.heightfield_rays(60000, n=64, seed=42)
+    fields = ("hit", "id", "t", "uv")
+    ref = psyref.RefScene(scene=sc).trace(rays, threads=8)
+    ctx.upload(sc)
+    host_tree = api.Tracer(ctx).trace(rays, fields=fields)
+    ctx.upload(sc, gpu_bvh=True)
+    st = ctx.stats()
+    dev_tree = api.Tracer(ctx).trace(rays, fields=fields)
+    assert st["bvh4_nodes"] > 0
+    for mine in (host_tree, dev_tree):
+        rep = parity.compare_trace(ref, mine, rays["type"])
+        parity.assert_parity(rep)
+    assert (host_tree["hit"] == dev_tree["hit"]).all()
+    # a device-built tree renders the same image as the host-built one, up to exact ties
+    from psychopath_cpp_b200 import api as A
+    ctx.upload(sc)
+    a, _ = A.PathTraceIntegrator(ctx, 64, 48, 4, seed=1, path_length=4).integrate()
+    ctx.upload(sc, gpu_bvh=True)
+    b, _ = A.PathTraceIntegrator(ctx, 64, 48, 4, seed=1, path_length=4).integrate()
+    m = a[..., 1] > 0
+    assert np.abs(a[..., 1][m] - b[..., 1][m]).max() <= 1e-5 * a[..., 1].max()
