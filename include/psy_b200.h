@@ -69,7 +69,9 @@ enum {
 	PSY_OBJ_SPHERE = 0,       /* data: n0 time samples of (cx cy cz r)            */
 	PSY_OBJ_BILINEAR = 1,     /* data: n0 time samples of 4 verts (12 floats)     */
 	PSY_OBJ_BICUBIC = 2,      /* data: n0 time samples of 16 verts (48 floats)    */
-	PSY_OBJ_SPHERE_LIGHT = 3  /* data: n0 positions (3), n1 radii, n2 colours (3) */
+	PSY_OBJ_SPHERE_LIGHT = 3, /* data: n0 positions (3), n1 radii, n2 colours (3) */
+	PSY_OBJ_RECT_LIGHT = 4    /* data: n0 dimensions (x y), n1 colours (3); in its xy plane at the origin
+	                             (RectangleLight, lights/rectangle_light.hpp) */
 };
 
 enum { PSY_INSTANCE_OBJECT = 0, PSY_INSTANCE_ASSEMBLY = 1 };

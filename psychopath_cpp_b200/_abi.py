@@ -20,7 +20,7 @@ PSY_ERR_STACK_OVERFLOW = -5
 PSY_ERR_NAN = -6
 PSY_ERR_NO_SCENE = -7
 
-PSY_OBJ_SPHERE, PSY_OBJ_BILINEAR, PSY_OBJ_BICUBIC, PSY_OBJ_SPHERE_LIGHT = 0, 1, 2, 3
+PSY_OBJ_SPHERE, PSY_OBJ_BILINEAR, PSY_OBJ_BICUBIC, PSY_OBJ_SPHERE_LIGHT, PSY_OBJ_RECT_LIGHT = 0, 1, 2, 3, 4
 PSY_INSTANCE_OBJECT, PSY_INSTANCE_ASSEMBLY = 0, 1
 PSY_SHADER_LAMBERT, PSY_SHADER_EMIT, PSY_SHADER_GTR = 0, 1, 2
 PSY_RAY_CAMERA, PSY_RAY_DIFFUSE, PSY_RAY_OCCLUSION = 1, 2, 32

@@ -18,7 +18,8 @@ from typing import Dict, List, Optional, Tuple
 import numpy as np
 
 from . import _abi
-from .scene import (Assembly, BicubicPatch, BilinearPatch, Scene, Sphere, SphereLight, SurfaceShader)
+from .scene import (Assembly, BicubicPatch, BilinearPatch, RectangleLight, Scene, Sphere, SphereLight,
+                    SurfaceShader)
 
 F32 = np.float32
 
@@ -84,6 +85,9 @@ def flatten(scene: Scene):
                 data = np.concatenate([ob.locations.ravel(), ob.radii.ravel(), ob.colors.ravel()]).astype(F32)
                 kind, n0, n1, n2 = (_abi.PSY_OBJ_SPHERE_LIGHT, ob.locations.shape[0], ob.radii.shape[0],
                                     ob.colors.shape[0])
+            elif isinstance(ob, RectangleLight):
+                data = np.concatenate([ob.dimensions.ravel(), ob.colors.ravel()]).astype(F32)
+                kind, n0, n1, n2 = _abi.PSY_OBJ_RECT_LIGHT, ob.dimensions.shape[0], ob.colors.shape[0], 0
             else:
                 raise TypeError("unsupported object %r" % type(ob))
             data = np.ascontiguousarray(data)

@@ -319,7 +319,7 @@ static int diff_params(psy_ctx* ctx, const psy_diff_desc* d, const char* who, Re
 	for (size_t i = 0; i < no; ++i) {
 		const int p = d->object_param[i];
 		if (p < -1 || p >= pc) return ctx_fail(ctx, PSY_ERR_ARG, "%s: object %zu's parameter %d is out of range", who, i, p);
-		if (p >= 0 && ctx->host->objects[i].kind != OBJ_SPHERE_LIGHT)
+		if (p >= 0 && ctx->host->objects[i].kind != OBJ_SPHERE_LIGHT && ctx->host->objects[i].kind != OBJ_RECT_LIGHT)
 			return ctx_fail(ctx, PSY_ERR_ARG, "%s: object %zu is not a light", who, i);
 	}
 	int rc;

@@ -23,7 +23,7 @@
 
 namespace psy {
 
-enum : int { OBJ_SPHERE = 0, OBJ_BILINEAR = 1, OBJ_BICUBIC = 2, OBJ_SPHERE_LIGHT = 3 };
+enum : int { OBJ_SPHERE = 0, OBJ_BILINEAR = 1, OBJ_BICUBIC = 2, OBJ_SPHERE_LIGHT = 3, OBJ_RECT_LIGHT = 4 };
 enum : int { INST_OBJECT = 0, INST_ASSEMBLY = 1 };
 enum : int { SHADER_LAMBERT = 0, SHADER_EMIT = 1, SHADER_GTR = 2 };
 enum : int { CLOSURE_NONE = 0, CLOSURE_LAMBERT = 1, CLOSURE_EMIT = 2, CLOSURE_GTR = 3 };

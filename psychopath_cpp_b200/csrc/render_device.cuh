@@ -487,6 +487,64 @@ static __device__ void sphere_light_sample(const DevScene& sc, const DevObject& 
 	*spec = rgb_to_spec(c, wl);
 }
 
+// uniform_sample_spherical_triangle (utils/monte_carlo.hpp:143-196, after
+// Arvo, "Stratified Sampling of Spherical Triangles", 1995): the angles in
+// double as there; the vector arithmetic is Vec3's float arithmetic, each
+// double factor rounded to float where it scales a Vec3.
+static __device__ V3 uniform_sample_spherical_triangle(V3 A, V3 B, V3 C, float i, float j) {
+	auto clampd = [](double v) { return fmin(1.0, fmax(-1.0, v)); };
+	const double cos_a = clampd((double)dot(B, C));
+	const double cos_b = clampd((double)dot(C, A));
+	const double cos_c = clampd((double)dot(A, B));
+	const double sin_a = sqrt(1.0 - (cos_a * cos_a));
+	const double sin_b = sqrt(1.0 - (cos_b * cos_b));
+	const double sin_c = sqrt(1.0 - (cos_c * cos_c));
+	if (cos_a == 1.0 || cos_b == 1.0 || cos_c == 1.0) return A;
+	const double cos_A = clampd((cos_a - (cos_b * cos_c)) / (sin_b * sin_c));
+	const double cos_B = clampd((cos_b - (cos_c * cos_a)) / (sin_c * sin_a));
+	const double cos_C = clampd((cos_c - (cos_a * cos_b)) / (sin_a * sin_b));
+	const double sin_A = sqrt(1.0 - (cos_A * cos_A));
+	const double ang_A = acos(cos_A);
+	const double ang_B = acos(cos_B);
+	const double ang_C = acos(cos_C);
+	const double area = ((ang_A + ang_B) + ang_C) - PSY_PI_D;
+	const double area_2 = area * (double)i;
+	const double s = sin(area_2 - ang_A);
+	const double t = cos(area_2 - ang_A);
+	const double u = t - cos_A;
+	const double v = s + (sin_A * cos_c);
+	const double q_top = (((v * t) - (u * s)) * cos_A) - v;
+	const double q_bottom = ((v * s) + (u * t)) * sin_A;
+	const double q = q_top / q_bottom;
+	const V3 C_2 = (A * (float)q) + (normalized(C - (A * dot(C, A))) * (float)sqrt(1.0 - (q * q)));
+	const double z = 1.0 - ((double)j * (1.0 - (double)dot(C_2, B)));
+	return (B * (float)z) + (normalized(C_2 - (B * dot(C_2, B))) * (float)sqrt(1.0 - (z * z)));
+}
+
+// RectangleLight::sample (lights/rectangle_light.hpp:40-71): one of the
+// rectangle's two spherical triangles, chosen by solid angle, sampled
+// uniformly and projected back onto the rectangle.
+static __device__ void rect_light_sample(const DevScene& sc, const DevObject& ob, V3 arr, float u, float v, float wl,
+                                         float time, V3* shadow_vec, float* pdf, Spec* spec) {
+	float dx, dy, col[3];
+	rect_light_at(sc, ob, time, &dx, &dy, col);
+	const double inv_surface_area = 1.0 / (double)(dx * dy);
+	V3 p[4];
+	float area_1, area_2;
+	rect_light_corners(dx, dy, arr, p, &area_1, &area_2);
+	const float prob_1 = area_1 / (area_1 + area_2);
+	const float prob_2 = 1.0f - prob_1;
+	V3 sv;
+	if (u < prob_1) sv = uniform_sample_spherical_triangle(p[1], p[0], p[2], v, u / prob_1);
+	else sv = uniform_sample_spherical_triangle(p[3], p[0], p[2], v, 1.0f - ((u - prob_1) / prob_2));
+	sv = sv * (-arr.z / sv.z);
+	*shadow_vec = sv;
+	*pdf = 1.0f / (area_1 + area_2);
+	const float isa = (float)inv_surface_area;
+	const float c[3] = {(col[0] * isa) * 0.5f, (col[1] * isa) * 0.5f, (col[2] * isa) * 0.5f};
+	*spec = rgb_to_spec(c, wl);
+}
+
 // LightTree::sample starting at the root assembly's tree.
 static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, float ident_inv) {
 	q->valid = false;
@@ -533,11 +591,14 @@ static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, floa
 		}
 		if (inst.kind == INST_OBJECT) {
 			const DevObject ob = sc.objects[inst.data];
-			if (ob.kind != OBJ_SPHERE_LIGHT) return;
+			if (ob.kind != OBJ_SPHERE_LIGHT && ob.kind != OBJ_RECT_LIGHT) return;
 			q->obj = inst.data;
 			float p = 1.0f;
 			V3 tl;
-			sphere_light_sample(sc, ob, q->pos, q->u, q->v, q->wavelength, q->time, &tl, &p, &q->spec);
+			if (ob.kind == OBJ_SPHERE_LIGHT)
+				sphere_light_sample(sc, ob, q->pos, q->u, q->v, q->wavelength, q->time, &tl, &p, &q->spec);
+			else
+				rect_light_sample(sc, ob, q->pos, q->u, q->v, q->wavelength, q->time, &tl, &p, &q->spec);
 			// xform.dir_from: the reference inverts the accumulated transform,
 			// which is the identity when no instance carried one
 			if (q->has_xform) q->to_light = dir_from(q->xform, tl, sc.rcp);

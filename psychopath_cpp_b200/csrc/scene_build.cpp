@@ -186,11 +186,13 @@ struct Builder {
 					case PSY_OBJ_BILINEAR: nfl = (size_t)od.n0 * 12; break;
 					case PSY_OBJ_BICUBIC: nfl = (size_t)od.n0 * 48; break;
 					case PSY_OBJ_SPHERE_LIGHT: nfl = (size_t)od.n0 * 3 + od.n1 + (size_t)od.n2 * 3; break;
+					case PSY_OBJ_RECT_LIGHT: nfl = (size_t)od.n0 * 2 + (size_t)od.n1 * 3; break;
 					default: return fail("unknown object kind " + std::to_string(od.kind));
 				}
 				if (od.n0 == 0) return fail("object with zero time samples");
 				if (od.kind == PSY_OBJ_SPHERE_LIGHT && (od.n1 == 0 || od.n2 == 0))
 					return fail("sphere light needs at least one radius and one colour");
+				if (od.kind == PSY_OBJ_RECT_LIGHT && od.n1 == 0) return fail("rectangle light needs at least one colour");
 				if (!od.data) return fail("object data pointer is NULL");
 				for (size_t k = 0; k < nfl; ++k) {
 					if (!std::isfinite(od.data[k])) return fail("non-finite object data");
@@ -222,6 +224,22 @@ struct Builder {
 							b.hi.at(k) += 0.0f;
 						}
 						ho.bounds.push_back(b);
+					}
+				} else if (od.kind == PSY_OBJ_RECT_LIGHT) {
+					// RectangleLight's bounds (lights/rectangle_light.hpp:28-35):
+					// the rectangle in its xy plane, one box per dimension sample
+					for (uint32_t t = 0; t < od.n0; ++t) {
+						const V3 dim3(p[t * 2] * 0.5f, p[t * 2 + 1] * 0.5f, 0.0f);
+						Box b;
+						b.lo = V3(0.0f) - dim3;
+						b.hi = V3(0.0f) + dim3;
+						ho.bounds.push_back(b);
+					}
+					// total_emitted_color = lerp_seq(0, colours) = the first colour
+					const float* col = p + od.n0 * 2;
+					for (int k = 0; k < 3; ++k) ho.emit[k] = col[k];
+					if (od.n1 > 1) {
+						for (int k = 0; k < 3; ++k) ho.emit[k] = (col[k] * one_minus(0.0f)) + (col[3 + k] * 0.0f);
 					}
 				} else {
 					std::vector<V3> pos;

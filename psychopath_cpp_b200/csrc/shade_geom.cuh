@@ -134,6 +134,43 @@ __device__ __forceinline__ float sphere_light_pdf(V3 pos, float radius_f, V3 arr
 	return (float)(1.0f / (4.0f * PSY_PI_D));
 }
 
+// spherical_triangle_solid_angle (utils/monte_carlo.hpp:110-137), in double
+// as there.
+__device__ __forceinline__ float spherical_triangle_solid_angle(V3 A, V3 B, V3 C) {
+	auto clampd = [](double v) { return fmin(1.0, fmax(-1.0, v)); };
+	const double cos_a = clampd((double)dot(B, C));
+	const double cos_b = clampd((double)dot(C, A));
+	const double cos_c = clampd((double)dot(A, B));
+	const double sin_a = sqrt(1.0 - (cos_a * cos_a));
+	const double sin_b = sqrt(1.0 - (cos_b * cos_b));
+	const double sin_c = sqrt(1.0 - (cos_c * cos_c));
+	if (cos_a == 1.0 || cos_b == 1.0 || cos_c == 1.0) return 0.0f;
+	const double cos_A = clampd((cos_a - (cos_b * cos_c)) / (sin_b * sin_c));
+	const double cos_B = clampd((cos_b - (cos_c * cos_a)) / (sin_c * sin_a));
+	const double cos_C = clampd((cos_c - (cos_a * cos_b)) / (sin_a * sin_b));
+	return (float)(((acos(cos_A) + acos(cos_B)) + acos(cos_C)) - PSY_PI_D);
+}
+
+// The four corners of a rectangle light (dimensions dx, dy), seen from
+// `arr` and projected on the unit sphere around it, and the solid angles of
+// its two triangles (lights/rectangle_light.hpp:48-57).
+__device__ __forceinline__ void rect_light_corners(float dx, float dy, V3 arr, V3 p[4], float* area_1, float* area_2) {
+	p[0] = normalized(V3(dx * 0.5f, dy * 0.5f, 0.0f) - arr);
+	p[1] = normalized(V3(dx * -0.5f, dy * 0.5f, 0.0f) - arr);
+	p[2] = normalized(V3(dx * -0.5f, dy * -0.5f, 0.0f) - arr);
+	p[3] = normalized(V3(dx * 0.5f, dy * -0.5f, 0.0f) - arr);
+	*area_1 = spherical_triangle_solid_angle(p[1], p[0], p[2]);
+	*area_2 = spherical_triangle_solid_angle(p[3], p[0], p[2]);
+}
+
+// RectangleLight::sample_pdf (lights/rectangle_light.hpp:73-88).
+__device__ __forceinline__ float rect_light_pdf(float dx, float dy, V3 arr) {
+	V3 p[4];
+	float a1, a2;
+	rect_light_corners(dx, dy, arr, p, &a1, &a2);
+	return 1.0f / (a1 + a2);
+}
+
 __device__ __forceinline__ void closure_of_shader(const DevScene& sc, int shader, HitInfo* h) {
 	if (shader < 0) {
 		h->closure = CLOSURE_EMIT;
@@ -204,6 +241,25 @@ static __device__ void hit_geometry(const DevScene& sc, const HitRec& rec, float
 		h->col[0] = col[0] / sa;
 		h->col[1] = col[1] / sa;
 		h->col[2] = col[2] / sa;
+	} else if (ob.kind == OBJ_RECT_LIGHT) {
+		// RectangleLight::intersect_ray's Intersection (lights/rectangle_light.hpp:122-135)
+		float dx, dy, col[3];
+		rect_light_at(sc, ob, time, &dx, &dy, col);
+		Geo& g = h->geo;
+		const float x = lo.x + (ld.x * t);
+		const float y = lo.y + (ld.y * t);
+		g.p = V3(x, y, 0.0f);
+		g.n = V3(0.0f, 0.0f, 1.0f);
+		g.u = g.v = 0.0f;
+		g.dpdu = g.dpdv = g.dndu = g.dndv = V3(0.0f);
+		h->backfacing = ld.z > 0.0f;
+		h->light_pdf = rect_light_pdf(dx, dy, lo);
+		h->offset = g.n * 0.000001f;
+		h->closure = CLOSURE_EMIT;
+		const float sa = (float)((double)(dx * dy));
+		h->col[0] = (col[0] * 0.5f) / sa;
+		h->col[1] = (col[1] * 0.5f) / sa;
+		h->col[2] = (col[2] * 0.5f) / sa;
 	} else {
 		Geo& g = h->geo;
 		g.p = lo + (ld * t);

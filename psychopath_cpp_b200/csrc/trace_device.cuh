@@ -202,6 +202,49 @@ __device__ __forceinline__ void light_at(const DevScene& sc, const DevObject& ob
 	}
 }
 
+// RectangleLight's dimensions and colour at `time` (lerp_seq over each
+// sequence, lights/rectangle_light.hpp:44-46).
+__device__ __forceinline__ void rect_light_at(const DevScene& sc, const DevObject& ob, float time, float* dx, float* dy,
+                                              float col[3]) {
+	const float* p = sc.fpool + ob.data;
+	{
+		const SeqPos sp = seq_pos(time, ob.n0);
+		const float* a = p + sp.i0 * 2;
+		if (sp.single) {
+			*dx = a[0];
+			*dy = a[1];
+		} else {
+			*dx = lerp1(sp.nalpha, a[0], a[2]);
+			*dy = lerp1(sp.nalpha, a[1], a[3]);
+		}
+	}
+	if (col) {
+		const float* cp = p + ob.n0 * 2;
+		const SeqPos sp = seq_pos(time, ob.n1);
+		const float* a = cp + sp.i0 * 3;
+		if (sp.single) {
+			col[0] = a[0]; col[1] = a[1]; col[2] = a[2];
+		} else {
+			const float ia = one_minus(sp.nalpha);
+			for (int k = 0; k < 3; ++k) col[k] = (a[k] * ia) + (a[3 + k] * sp.nalpha);
+		}
+	}
+}
+
+// RectangleLight::intersect_ray's hit test (lights/rectangle_light.hpp:
+// 106-121): the plane z = 0 of the light's space, inside the rectangle.
+// The upper y bound is dimension x / 2, as the reference has it.  Returns t
+// or -1.
+__device__ __forceinline__ float rect_light_t(V3 o, V3 d, V3 dinv, float dx, float dy, float max_t) {
+	if (d.z == 0.0f) return -1.0f;
+	const float t = -o.z * dinv.z;
+	if (t <= 0.0f || t > max_t) return -1.0f;
+	const float x = o.x + (d.x * t);
+	const float y = o.y + (d.y * t);
+	if (x >= (dx * -0.5f) && x <= (dx * 0.5f) && y >= (dy * -0.5f) && y <= (dx * 0.5f)) return t;
+	return -1.0f;
+}
+
 // ---------------------------------------------------------------------
 // Patches (object/bilinear.hpp, object/bicubic.hpp)
 // ---------------------------------------------------------------------
@@ -1227,6 +1270,15 @@ __device__ __forceinline__ bool object_test(const DevScene& sc, TraceState<F>& s
 			light_at(sc, ob, wr.time, &cent, &radi, col);
 		}
 		const float t = sphere_t(lr.o, lr.d, cent, radi, max_t);
+		if (t >= 0.0f) {
+			hit = true;
+			ph.t = t;
+			if (!wr.occl) max_t = t;
+		}
+	} else if (ob.kind == OBJ_RECT_LIGHT) {
+		float dx, dy;
+		rect_light_at(sc, ob, wr.time, &dx, &dy, nullptr);
+		const float t = rect_light_t(lr.o, lr.d, lr.dinv, dx, dy, max_t);
 		if (t >= 0.0f) {
 			hit = true;
 			ph.t = t;

@@ -122,7 +122,21 @@ class SphereLight:
         self.colors = _f32(self.colors).reshape(-1, 3)
 
 
-SceneObject = Union[Sphere, BilinearPatch, BicubicPatch, SphereLight]
+@dataclass
+class RectangleLight:
+    """Rectangle light in its local xy plane, centred on the origin, with
+    per-time-sample dimensions (x, y) and colours (reference
+    lights/rectangle_light.hpp:16-40, parser/parser.cpp:597-632)."""
+
+    dimensions: np.ndarray
+    colors: np.ndarray
+
+    def __post_init__(self):
+        self.dimensions = _f32(self.dimensions).reshape(-1, 2)
+        self.colors = _f32(self.colors).reshape(-1, 3)
+
+
+SceneObject = Union[Sphere, BilinearPatch, BicubicPatch, SphereLight, RectangleLight]
 
 
 @dataclass
@@ -284,6 +298,13 @@ class Scene:
                     w("%s\tRadius [%s]\n" % (ind2, fmt_f32(r)))
                 for loc in obj.locations:
                     w("%s\tLocation [%s]\n" % (ind2, _fmt_list(loc)))
+                w("%s}\n" % ind2)
+            elif isinstance(obj, RectangleLight):
+                w("%sRectangleLight $%s {\n" % (ind2, oname))
+                for c in obj.colors:
+                    w("%s\tColor [%s]\n" % (ind2, _fmt_list(c)))
+                for d in obj.dimensions:
+                    w("%s\tDimensions [%s]\n" % (ind2, _fmt_list(d)))
                 w("%s}\n" % ind2)
             else:
                 raise TypeError("unsupported object %r" % (type(obj),))
@@ -485,6 +506,15 @@ def _parse_assembly(node: _Node, parent: Optional[Assembly]) -> Assembly:
             if not locs:
                 locs = [_f32([0, 0, 0])]
             asm.add_object(ch.name[1:], SphereLight(np.array(locs), np.array(rads, dtype=np.float32), np.array(cols)))
+        elif t == "RectangleLight":
+            cols, dims = [], []
+            for c in ch.children:
+                if c.type == "Color":
+                    cols.append(_color(c.leaf))
+                elif c.type == "Dimensions":
+                    v = _floats(c.leaf, 2)
+                    dims.append([v[0] if len(v) > 0 else 1.0, v[1] if len(v) > 1 else 1.0])
+            asm.add_object(ch.name[1:], RectangleLight(np.array(dims, dtype=np.float32), np.array(cols)))
         elif t == "Instance":
             data, xf, shader = "", [], None
             for c in ch.children:

@@ -113,6 +113,32 @@ def adjoint_scene(seed: int = 1, res=(256, 256), spp: int = 32, n_spheres: int =
     return sc
 
 
+def rect_light_scene(seed: int = 1, res=(96, 72), spp: int = 16, n_spheres: int = 24) -> Scene:
+    """The plain scene's geometry lit by rectangle lights instead of a
+    sphere light: one overhead (3 x 1.5, facing down through an instance
+    transform), one tilted panel (1 x 2.5) to the side, with the
+    reference's own rectangle-light arithmetic, including its upper y bound
+    of half the x dimension."""
+    from .scene import RectangleLight
+    rng = np.random.default_rng(seed)
+    sc = Scene(name="rect_light_%d" % seed, res_x=res[0], res_y=res[1], spp=spp, seed=1)
+    sc.camera = Camera(transforms=[look_at((0.0, -15.0, 7.0), (0.0, 0.0, 0.5))], fovs=[45.0])
+    root = sc.root
+    root.add_shader("ground_mat", SurfaceShader("Lambert", [0.6, 0.55, 0.5]))
+    root.add_object("ground", BilinearPatch([[-10, -10, 0], [10, -10, 0], [-10, 10, 0], [10, 10, 0]]))
+    root.add_instance("ground", shader="ground_mat")
+    for i in range(n_spheres):
+        root.add_shader("mat%d" % i, SurfaceShader("Lambert", [rng.uniform(0.2, 0.8)] * 3))
+        root.add_object("sphere%d" % i, Sphere([rng.uniform(-5, 5), rng.uniform(-5, 5), rng.uniform(0, 2)],
+                                               rng.uniform(0.2, 0.6)))
+        root.add_instance("sphere%d" % i, shader="mat%d" % i)
+    root.add_object("panel", RectangleLight([[3.0, 1.5]], [[60.0, 60.0, 55.0]]))
+    root.add_instance("panel", [placement((1.0, 0.0, 0.0), math.pi, (0.0, 0.0, 6.0))])
+    root.add_object("side", RectangleLight([[1.0, 2.5]], [[30.0, 35.0, 40.0]]))
+    root.add_instance("side", [placement((0.3, 1.0, 0.2), 1.2, (-4.0, 2.0, 3.0))])
+    return sc
+
+
 # --------------------------------------------------------------------------
 # Heightfield trace microbenchmark
 # --------------------------------------------------------------------------

@@ -123,3 +123,30 @@ def test_render_rejects_bad_arguments(ctx):
         api.PathTraceIntegrator(ctx, 0, 8, 1).integrate()
     with pytest.raises(Exception):
         api.PathTraceIntegrator(ctx, 8, 8, 0).integrate()
+
+
+def test_rect_light_render(ctx, ref_available):
+    """Rectangle lights (RectangleLight, lights/rectangle_light.hpp): hits,
+    light-tree sampling of spherical triangles and MIS, one light placed by
+    an instance transform."""
+    sc = scenes.rect_light_scene(1, res=(96, 72), spp=16)
+    (rx, rc, rrays), (mx, mc, mrays) = _render_both(ctx, sc, 16, 4)
+    assert (rc == mc).all()
+    err, npx = rel_rmse(mx, rx)
+    assert npx > 3000
+    assert err <= IMAGE_REL_RMSE, err
+    assert abs(int(rrays) - int(mrays)) <= 0.001 * rrays, (rrays, mrays)
+
+
+def test_rect_light_sample_parity(ctx, ref_available):
+    from oracle import psyref
+    sc = scenes.rect_light_scene(2)
+    q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 3), 3)
+    ref_out, ref_ids = psyref.RefScene(scene=sc).light_sample(q)
+    ctx.upload(sc)
+    out, ids = api.LightTree(ctx).sample(q)
+    same = ref_ids == ids
+    assert same.mean() > 0.999, same.mean()
+    for name, sl in (("to_light", slice(0, 3)), ("spec", slice(3, 7)), ("light_pdf", slice(9, 10))):
+        d = parity.ulp_diff(ref_out[same, sl], out[same, sl])
+        assert np.percentile(d, 99) <= 8, (name, np.percentile(d, 99), int(d.max()))

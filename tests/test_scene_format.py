@@ -20,7 +20,8 @@ def test_float_formatting_round_trips_through_float32():
                                   lambda: scenes.heightfield_scene(8),
                                   lambda: scenes.many_light_scene(2, res=(32, 18), spp=2, n_patches=12,
                                                                   n_groups=10, n_lights=20),
-                                  lambda: scenes.motion_patch_scene(1, n=3)])
+                                  lambda: scenes.motion_patch_scene(1, n=3),
+                                  lambda: scenes.rect_light_scene(1, res=(8, 6), spp=1, n_spheres=3)])
 def test_write_parse_round_trip(make):
     sc = make()
     txt = sc.to_psy()

@@ -223,3 +223,32 @@ def test_device_built_bvh_gives_the_same_hits(ctx, ref_available, kind):
     b, _ = A.PathTraceIntegrator(ctx, 64, 48, 4, seed=1, path_length=4).integrate()
     m = a[..., 1] > 0
     assert np.abs(a[..., 1][m] - b[..., 1][m]).max() <= 1e-5 * a[..., 1].max()
+
+
+def test_rect_light_hits(ctx, ref_available):
+    """Rays against rectangle lights: hit, id and t exact-to-4-ulp, the
+    emission closure colour and light pdf of the light hits."""
+    from oracle import psyref
+    sc = scenes.rect_light_scene(3)
+    rng = np.random.default_rng(8)
+    n = 40000
+    o = np.stack([rng.uniform(-5, 5, n), rng.uniform(-5, 5, n), rng.uniform(0.5, 3.0, n)], 1)
+    tgt = np.where(rng.uniform(0, 1, (n, 1)) < 0.5,
+                   np.stack([rng.uniform(-2, 2, n), rng.uniform(-1.5, 1.5, n), np.full(n, 6.0)], 1),
+                   np.stack([rng.uniform(-5, -3, n), rng.uniform(1, 3, n), rng.uniform(2, 4, n)], 1))
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = {"o": o.astype(np.float32), "d": d.astype(np.float32), "odx": np.zeros((n, 3), np.float32),
+            "ody": np.zeros((n, 3), np.float32), "ddx": np.zeros((n, 3), np.float32),
+            "ddy": np.zeros((n, 3), np.float32), "time": rng.uniform(0, 1, n).astype(np.float32),
+            "type": np.full(n, 2, np.uint16)}
+    ref = psyref.RefScene(scene=sc).trace(rays, threads=8)
+    ctx.upload(sc)
+    mine = api.Tracer(ctx).trace(rays, fields=("hit", "id", "t", "closure", "closure_color", "light_pdf"))
+    rep = parity.compare_trace(ref, mine, rays["type"])
+    parity.assert_parity(rep)
+    light = (mine["hit"] == 1) & (mine["closure"] == 2)
+    assert light.sum() > 2000
+    out = ref["out"]
+    assert parity.ulp_diff(out[light, 43:46], mine["closure_color"][light]).max() == 0
+    assert np.percentile(parity.ulp_diff(out[light, 22], mine["light_pdf"][light]), 99) <= 8
