@@ -81,6 +81,7 @@ struct PathSoA {
 	float4* lcol;       // between the shadow ray and its result: the light's contribution
 	float* hit;         // stored intersection, 16 floats per path
 	float* pray;        // previous ray, 16 floats per path
+	float* hitx;        // GTR hits: world dpdu, dpdv, dndu, dndv, 12 floats per path
 	float* sample;      // film sample XYZ, 3 floats per path
 	uint16_t* rid;      // render of the path (batches)
 	// adjoint pass only

@@ -114,12 +114,6 @@ static int check_render(psy_ctx* ctx, const psy_render_desc* desc, const char* w
 	if (desc->path_length > 40) return ctx_fail(ctx, PSY_ERR_ARG, "%s: path_length must be at most 40", who);
 	if (ctx->host->assemblies[0].light_root < 0)
 		return ctx_fail(ctx, PSY_ERR_ARG, "%s: the scene has no lights (the reference integrator needs one)", who);
-	// The trace reports GTR closures (Intersection::surface_closure), but the
-	// wave kernels shade Lambert and emission only: refuse rather than end
-	// such paths early.
-	for (size_t i = 0; i < ctx->host->shaders.size(); ++i)
-		if (ctx->host->shaders[i].kind == SHADER_GTR)
-			return ctx_fail(ctx, PSY_ERR_ARG, "%s: shader %zu is GTR, which the renderer does not shade", who, i);
 	return PSY_OK;
 }
 
@@ -176,6 +170,7 @@ static int wave_set(psy_ctx* ctx, const char* prefix, uint64_t P, uint32_t path_
 	ps.lcol = (float4*)buf("lcol", P * 16);
 	ps.hit = (float*)buf("hit", P * 64);
 	ps.pray = (float*)buf("pray", P * 64);
+	ps.hitx = (float*)buf("hitx", P * 48);
 	ps.sample = (float*)buf("sample", P * 12);
 	ps.rid = (uint16_t*)buf("rid", P * 2);
 	ps.adj = nullptr;
@@ -209,7 +204,7 @@ static int wave_set(psy_ctx* ctx, const char* prefix, uint64_t P, uint32_t path_
 	wb.hit_i = (int4*)buf("hiti", P * 48);
 	wb.occl = (uint8_t*)buf("occl", P);
 	if (!ps.smp || !ps.dimstep || !ps.wl || !ps.time || !ps.last_pdf || !ps.col || !ps.fcol || !ps.lcol ||
-	    !ps.hit || !ps.pray || !ps.sample || !ps.rid || !wq.q0 || !wq.q1 || !wq.counters || !wq.rays || !wb.ray[0] ||
+	    !ps.hit || !ps.pray || !ps.hitx || !ps.sample || !ps.rid || !wq.q0 || !wq.q1 || !wq.counters || !wq.rays || !wb.ray[0] ||
 	    !wb.ray[1] || !wb.hit_f || !wb.hit_i || !wb.occl)
 		return rc ? rc : PSY_ERR_OOM;
 	return PSY_OK;

@@ -110,8 +110,13 @@ struct alignas(16) DevLightNode {
 struct alignas(16) DevShader {
 	int kind;
 	float col[3];
-	float roughness, tail_shape, fresnel;
-	int pad;
+	// GTR: the parameters as GTRClosure::validate leaves them
+	// (shading/surface_closure.hpp:352-372), its normalisation factor, and
+	// pow(roughness^2, 1 - tail_shape); both computed on the host with the
+	// host's powf, as the reference computes them
+	float roughness, tail_shape, fresnel, norm;
+	float pow_r2_1mt;
+	int pad[3];
 };
 
 // Device pointers of an uploaded scene, passed to kernels by value.

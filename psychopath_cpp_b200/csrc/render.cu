@@ -112,7 +112,9 @@ struct StoredHit {
 	float col[3];       // closure colour (Lambert)
 	int pid;            // differentiable renders: the shader's first albedo weight (>= 0), -2 - q when its
 	                    // RGB albedo is scaled by params[q], or -1 (not parameterised)
+	int gtr;            // the GTR shader of the hit, or -1 (Lambert)
 	V3 d, odx, ody, ddx, ddy;  // previous ray
+	V3 dpdu, dpdv, dndu, dndv; // GTR hits: geo's derivatives in world space (transformed_from)
 };
 
 __device__ __forceinline__ void load_hit(const PathSoA& ps, int s, StoredHit* h) {
@@ -125,6 +127,15 @@ __device__ __forceinline__ void load_hit(const PathSoA& ps, int s, StoredHit* h)
 	h->col[0] = c.z; h->col[1] = c.w; h->col[2] = d.x;
 	h->bf = d.y;
 	h->pid = __float_as_int(d.z);
+	h->gtr = __float_as_int(d.w);
+	if (h->gtr >= 0) {
+		const float4* x = reinterpret_cast<const float4*>(ps.hitx) + (size_t)s * 3;
+		const float4 u = x[0], v = x[1], w = x[2];
+		h->dpdu = V3(u.x, u.y, u.z);
+		h->dpdv = V3(u.w, v.x, v.y);
+		h->dndu = V3(v.z, v.w, w.x);
+		h->dndv = V3(w.y, w.z, w.w);
+	}
 	const float4* r = reinterpret_cast<const float4*>(ps.pray) + (size_t)s * 4;
 	const float4 e = r[0], f = r[1], gg = r[2], hh = r[3];
 	h->d = V3(e.x, e.y, e.z);
@@ -139,7 +150,13 @@ __device__ __forceinline__ void store_hit(const PathSoA& ps, int s, const Stored
 	g[0] = make_float4(h.p.x, h.p.y, h.p.z, h.n.x);
 	g[1] = make_float4(h.n.y, h.n.z, h.off.x, h.off.y);
 	g[2] = make_float4(h.off.z, h.t, h.col[0], h.col[1]);
-	g[3] = make_float4(h.col[2], h.bf, __int_as_float(h.pid), 0.0f);
+	g[3] = make_float4(h.col[2], h.bf, __int_as_float(h.pid), __int_as_float(h.gtr));
+	if (h.gtr >= 0) {
+		float4* x = reinterpret_cast<float4*>(ps.hitx) + (size_t)s * 3;
+		x[0] = make_float4(h.dpdu.x, h.dpdu.y, h.dpdu.z, h.dpdv.x);
+		x[1] = make_float4(h.dpdv.y, h.dpdv.z, h.dndu.x, h.dndu.y);
+		x[2] = make_float4(h.dndu.z, h.dndv.x, h.dndv.y, h.dndv.z);
+	}
 	float4* r = reinterpret_cast<float4*>(ps.pray) + (size_t)s * 4;
 	r[0] = make_float4(h.d.x, h.d.y, h.d.z, h.odx.x);
 	r[1] = make_float4(h.odx.y, h.odx.z, h.ody.x, h.ody.y);
@@ -165,7 +182,7 @@ __device__ void make_stored(const DevScene& sc, const HitRec& rec, const WorldRa
 	*closure = h.closure;
 	emit_col[0] = h.col[0]; emit_col[1] = h.col[1]; emit_col[2] = h.col[2];
 	*light_pdf = h.light_pdf;
-	if (h.closure != CLOSURE_LAMBERT) return;
+	if (h.closure != CLOSURE_LAMBERT && h.closure != CLOSURE_GTR) return;
 	M44 inv;
 	if (xf) {
 		inv = m44_inverse(space, sc.rcp);
@@ -174,9 +191,19 @@ __device__ void make_stored(const DevScene& sc, const HitRec& rec, const WorldRa
 		for (int i = 0; i < 4; ++i) inv.m[i][i] = ident_inv;
 	}
 	sh->p = pos_to(inv, h.geo.p);
-	const V3 n = xf ? nor_from(space, h.geo.n) : nor_from(m44_identity(), h.geo.n);
+	const M44 nx = xf ? space : m44_identity();
+	const V3 n = nor_from(nx, h.geo.n);
 	const float il = 1.0f / length(n);
 	sh->n = n * il;
+	sh->gtr = -1;
+	if (h.closure == CLOSURE_GTR) {
+		// the rest of DifferentialGeometry::transformed_from (basics/differential_geometry.hpp:20-40)
+		sh->gtr = rec.shader;
+		sh->dpdu = dir_to(inv, h.geo.dpdu);
+		sh->dpdv = dir_to(inv, h.geo.dpdv);
+		sh->dndu = nor_from(nx, h.geo.dndu) * il;
+		sh->dndv = nor_from(nx, h.geo.dndv) * il;
+	}
 	V3 off = dir_to(inv, h.offset);
 	if (h.backfacing) off = off * -1.0f;
 	sh->off = off;
@@ -202,6 +229,39 @@ __device__ __forceinline__ void propagate_differentials(const StoredHit& h, Worl
 	out->ody = transfer_origin_differential(h.t, nn, h.d, h.ody, h.ddy);
 	out->ddx = (x * 0.15f) / len;
 	out->ddy = (y * 0.15f) / len;
+}
+
+// GTRClosure::propagate_differentials (shading/surface_closure.hpp:574-607):
+// origin differentials transferred to the hit, normal differentials turned
+// into half-vector differentials, direction differentials reflected about
+// the half vector, then clamped (clamp_dd).
+__device__ void gtr_propagate_differentials(const StoredHit& h, WorldRayD* out) {
+	V3 nn = normalized(h.n);
+	const V3 hh = normalized(normalized(h.d * -1.0f) + normalized(out->d));
+	out->odx = transfer_origin_differential(h.t, nn, h.d, h.odx, h.ddx);
+	out->ody = transfer_origin_differential(h.t, nn, h.d, h.ody, h.ddy);
+	float dux, dvx, duy, dvy;
+	uv_differentials(out->odx, h.dpdu, h.dpdv, &dux, &dvx);
+	uv_differentials(out->ody, h.dpdu, h.dpdv, &duy, &dvy);
+	V3 dndx = (h.dndu * dux) + (h.dndv * dvx);
+	V3 dndy = (h.dndu * duy) + (h.dndv * dvy);
+	if (dot(nn, hh) < 0.0f) {
+		nn = nn * -1.0f;
+		dndx = dndx * -1.0f;
+		dndy = dndy * -1.0f;
+	}
+	const V3 axis = normalized(cross(nn, hh));
+	const float angle = acosf(clampf(dot(nn, hh), 0.0f, 1.0f));
+	const M44 xf = axis_angle(axis, angle);
+	const V3 dhdx = dir_to(xf, dndx);
+	const V3 dhdy = dir_to(xf, dndy);
+	out->ddx = reflect_dd(hh, dhdx, h.d, h.ddx);
+	out->ddy = reflect_dd(hh, dhdy, h.d, h.ddy);
+	const float len_d = length(out->d);
+	const float len_dx = length(out->ddx);
+	const float len_dy = length(out->ddy);
+	if ((len_dx / len_d) > 0.9f) out->ddx = out->ddx * ((0.9f * len_d) / len_dx);
+	if ((len_dy / len_d) > 0.9f) out->ddy = out->ddy * ((0.9f * len_d) / len_dy);
 }
 
 __device__ __forceinline__ void finish_path(const PathSoA& ps, int slot, const Spec& col, float wl) {
@@ -614,7 +674,7 @@ __global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathS
 						}
 						grad_add(rp, sgrad, ps, slot, vtx, B, lp, wl);
 					}
-				} else if (closure != CLOSURE_LAMBERT) {
+				} else if (closure != CLOSURE_LAMBERT && closure != CLOSURE_GTR) {
 					done = true;  // closures outside the supported set end the path
 				} else {
 					sh.pid = (rp.params && rec.shader >= 0) ? rp.shader_param[rec.shader] : -1;
@@ -639,8 +699,26 @@ __global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathS
 			}
 			step++;
 			if (step == rp.path_length * 2) done = true;
+			const bool gtr = !done && sh.gtr >= 0;
+			const Gtr gp = gtr ? gtr_of(sc.shaders[sh.gtr]) : Gtr{};
 			if (done) {
 				finish_path(ps, slot, col, wl);
+			} else if (gtr && gtr_is_delta(gp)) {
+				// a delta closure takes no light sample and no sampler draws;
+				// the reference traces the step's ray again, and its result
+				// adds nothing (path_trace_integrator.cpp:131-184, 235-249)
+				sray = wr;
+				sray.occl = true;
+				stag = rid << 1;
+				ps.dimstep[slot] = (dim & 0xffffu) | (step << 16);
+				ps.col[slot] = f4(col);
+				ps.lcol[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+				if (!W::BATCH && rp.grad) {
+					ps.nee_param[slot] = -1;
+					ps.nee_base[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+				}
+				store_hit(ps, slot, sh);
+				live = true;
 			} else {
 				// shadow step: light-tree sample and shadow ray
 				LightQuery q;
@@ -658,10 +736,12 @@ __global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathS
 				q.obj = -1;
 				q.selection_pdf = 1.0f;
 				q.light_sample_pdf = 1.0f;
+				q.gtr = gtr;
+				q.gp = gp;
 				light_tree_sample(sc, &q, rp.ident_inv);
 				float4 contrib = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 				if (q.valid) {
-					const float bsdf_pdf = lambert_pdf(sh.d, q.to_light, sh.n);
+					const float bsdf_pdf = gtr ? gtr_pdf(gp, sh.d, q.to_light, sh.n) : lambert_pdf(sh.d, q.to_light, sh.n);
 					const float mis_inv_pdf = power_heuristic(q.light_sample_pdf, bsdf_pdf) / q.light_sample_pdf;
 					const float lc = (float)rp.light_count;
 					Spec lcol;
@@ -674,17 +754,18 @@ __global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathS
 					sray.d = (q.to_light - sh.off) * 0.9995f;
 					sray.time = time;
 					sray.occl = true;
-					propagate_differentials(sh, &sray);
+					if (gtr) gtr_propagate_differentials(sh, &sray);
+					else propagate_differentials(sh, &sray);
 					// the light's contribution if the shadow ray is not blocked
 					// (update_path, shadow result: path_trace_integrator.cpp:235-249)
-					const Spec fac = lambert_eval_p(rp, sh, sray.d, wl);
+					const Spec fac = gtr ? gtr_eval(gp, sh.d, sray.d, sh.n, wl) : lambert_eval_p(rp, sh, sray.d, wl);
 					Spec c;
 					for (int k = 0; k < 4; ++k) c.e[k] = (fcol.e[k] * lcol.e[k]) * fac.e[k];
 					contrib = f4(c);
 					if (!W::BATCH && rp.grad) {
 						// without the light's scale and the albedos of parameterised vertices
 						const Spec fx = sp(ps.fexcl[slot]);
-						const float cs = lambert_cos(sh.d, sray.d, sh.n);
+						const float cs = gtr ? 0.0f : lambert_cos(sh.d, sray.d, sh.n);
 						const Spec f0 = sh.pid != -1 ? Spec{{cs, cs, cs, cs}} : fac;
 						Spec b;
 						for (int k = 0; k < 4; ++k)
@@ -770,25 +851,42 @@ __global__ void __launch_bounds__(256) shade_shadow_kernel(W w, HaltonDev hd, Pa
 		// first `sj`.
 		const float sj = sampler_get(hd, smp, dim++);
 		const float si = sampler_get(hd, smp, dim++);
-		V3 nn = normalized(sh.n);
-		if (dot(nn, sh.d) > 0.0f) nn = nn * -1.0f;
-		const V3 dir = cosine_sample_hemisphere(si, sj);
-		float pdf = dir.z * (float)PSY_INV_PI_D;
-		const V3 out = zup_to_vec(dir, nn);
-		const Spec filter = lambert_eval_p(rp, sh, out, wl);
 		WorldRayD wr;
 		wr.o = sh.p + sh.off;
-		wr.d = out;
 		wr.time = ps.time[slot];
 		wr.occl = false;
-		propagate_differentials(sh, &wr);
-		if (pdf < 0.00001f) pdf = 0.00001f;
-		for (int k = 0; k < 4; ++k) fcol.e[k] *= filter.e[k] / pdf;
+		V3 out;
+		float pdf;
+		Spec filter;
+		bool delta = false;
+		if (sh.gtr >= 0) {
+			const Gtr gp = gtr_of(w.scene(rid).shaders[sh.gtr]);
+			gtr_sample(gp, sh.d, sh.n, si, sj, wl, &out, &filter, &pdf);
+			delta = gtr_is_delta(gp);
+			wr.d = out;
+			gtr_propagate_differentials(sh, &wr);
+		} else {
+			V3 nn = normalized(sh.n);
+			if (dot(nn, sh.d) > 0.0f) nn = nn * -1.0f;
+			const V3 dir = cosine_sample_hemisphere(si, sj);
+			pdf = dir.z * (float)PSY_INV_PI_D;
+			out = zup_to_vec(dir, nn);
+			filter = lambert_eval_p(rp, sh, out, wl);
+			wr.d = out;
+			propagate_differentials(sh, &wr);
+		}
+		if (!delta) {
+			if (pdf < 0.00001f) pdf = 0.00001f;
+			for (int k = 0; k < 4; ++k) fcol.e[k] *= filter.e[k] / pdf;
+		} else {
+			for (int k = 0; k < 4; ++k) fcol.e[k] *= filter.e[k];
+			pdf = 0.0f;  // last_pdf 0: the next emitter hit takes no MIS weight
+		}
 		if (!W::BATCH && rp.grad) {
 			// the path weight without the parameterised albedos
 			Spec fx = sp(ps.fexcl[slot]);
-			const float cs = lambert_cos(sh.d, out, sh.n);
-			for (int k = 0; k < 4; ++k) fx.e[k] *= (sh.pid != -1 ? cs : filter.e[k]) / pdf;
+			const float cs = sh.gtr >= 0 ? 0.0f : lambert_cos(sh.d, out, sh.n);
+			for (int k = 0; k < 4; ++k) fx.e[k] *= (sh.pid != -1 ? cs : filter.e[k]) / (delta ? 1.0f : pdf);
 			ps.fexcl[slot] = f4(fx);
 		}
 		store_ray(wb.ray[0], wb.cap, i, wr, rid << 1);
@@ -971,6 +1069,7 @@ __global__ void light_sample_kernel(DevScene sc, LightQuerySoADev q, LightSample
 	lq.wavelength = q.wavelength[i];
 	lq.time = q.time[i];
 	lq.has_xform = false;
+	lq.gtr = false;
 	lq.id = 0;
 	lq.selection_pdf = 1.0f;
 	lq.light_sample_pdf = 1.0f;

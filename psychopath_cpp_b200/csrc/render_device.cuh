@@ -328,6 +328,185 @@ __device__ __forceinline__ float lambert_cos(V3 in, V3 out, V3 n) {
 }
 
 // ---------------------------------------------------------------------
+// GTR microfacet closure (GTRClosure, shading/surface_closure.hpp:339-608)
+// ---------------------------------------------------------------------
+// The closure's parameters at a hit (from its validated shader).
+struct Gtr {
+	float col[3];
+	float rough, tail, fres, norm, pow_r2_1mt;
+};
+
+__device__ __forceinline__ Gtr gtr_of(const DevShader& s) {
+	Gtr g;
+	g.col[0] = s.col[0]; g.col[1] = s.col[1]; g.col[2] = s.col[2];
+	g.rough = s.roughness;
+	g.tail = s.tail_shape;
+	g.fres = s.fresnel;
+	g.norm = s.norm;
+	g.pow_r2_1mt = s.pow_r2_1mt;
+	return g;
+}
+
+__device__ __forceinline__ bool gtr_is_delta(const Gtr& g) { return g.rough == 0.0f; }
+
+__device__ __forceinline__ float clampf(float v, float a, float b) { return smin(b, smax(a, v)); }
+
+// GTRClosure::normalization (:374-380): top in float, the division in double.
+__device__ __forceinline__ float gtr_normalization(float r, float t) {
+	const float r2 = r * r;
+	const float top = (t - 1.0f) * (r2 - 1.0f);
+	const double bottom = PSY_PI_D * (double)(1.0f - powf(r2, 1.0f - t));
+	return (float)((double)top / bottom);
+}
+
+// GTRClosure::dist (:397-409) with the normalisation factor `norm` of `rough`.
+__device__ __forceinline__ float gtr_dist(float nh, float rough, float tail, float norm) {
+	const float r2 = rough * rough;
+	float D = 0.0f;
+	if (nh > 0.0f) {
+		const float nh2 = nh * nh;
+		D = norm / powf(1.0f + ((r2 - 1.0f) * nh2), tail);
+	}
+	return D;
+}
+
+// GTRClosure::half_theta_sample (:383-395).
+__device__ __forceinline__ float gtr_half_theta_sample(const Gtr& g, float u) {
+	const float r2 = g.rough * g.rough;
+	const float top = 1.0f - powf((g.pow_r2_1mt * (1.0f - u)) + u, 1.0f / (1.0f - g.tail));
+	const float bottom = 1.0f - r2;
+	return sqrtf(top / bottom);
+}
+
+// schlick_fresnel_from_fac (:173-177).
+__device__ __forceinline__ float schlick_fresnel_from_fac(float f, float c) {
+	const float c1 = 1.0f - c;
+	const float c2 = c1 * c1;
+	return f + ((((1.0f - f) * c1) * c2) * c2);
+}
+
+// GTRClosure::evaluate (:452-516).
+__device__ __forceinline__ Spec gtr_eval(const Gtr& g, V3 in, V3 out, V3 n, float wl) {
+	V3 nn = normalized(n);
+	const V3 aa = normalized(in) * -1.0f;
+	const V3 bb = normalized(out);
+	const V3 hh = normalized(aa + bb);
+	if (dot(nn, hh) < 0.0f) nn = nn * -1.0f;
+	const float na = clampf(dot(nn, aa), -1.0f, 1.0f);
+	const float nb = clampf(dot(nn, bb), -1.0f, 1.0f);
+	const float ha = clampf(dot(hh, aa), -1.0f, 1.0f);
+	const float hb = clampf(dot(hh, bb), -1.0f, 1.0f);
+	const float nh = clampf(dot(nn, hh), -1.0f, 1.0f);
+	const float r2 = g.rough * g.rough;
+	float D = 1.0f, G1 = 1.0f, G2 = 1.0f;
+	Spec col_f = rgb_to_spec(g.col, wl);
+	for (int i = 0; i < 4; ++i) col_f.e[i] = lerp1(1.0f - g.fres, schlick_fresnel_from_fac(col_f.e[i], hb), col_f.e[i]);
+	if (g.rough == 0.0f) return col_f;
+	if (nh > 0.0f) {
+		const float nh2 = nh * nh;
+		D = g.norm / powf(1.0f + ((r2 - 1.0f) * nh2), g.tail);
+	}
+	const float na2 = na * na;
+	const float tan_na = sqrtf((1.0f - na2) / na2);
+	const float g1_pos_char = (ha * na) > 0.0f ? 1.0f : 0.0f;
+	const float g1_a = r2 * tan_na;
+	const float g1_b = (sqrtf(1.0f + (g1_a * g1_a)) - 1.0f) * 0.5f;
+	G1 = g1_pos_char / (1.0f + g1_b);
+	const float nb2 = nb * nb;
+	const float tan_nb = sqrtf((1.0f - nb2) / nb2);
+	const float g2_pos_char = (hb * nb) > 0.0f ? 1.0f : 0.0f;
+	const float g2_a = r2 * tan_nb;
+	const float g2_b = (sqrtf(1.0f + (g2_a * g2_a)) - 1.0f) * 0.5f;
+	G2 = g2_pos_char / (1.0f + g2_b);
+	const float f = (D * G1) * G2;
+	for (int i = 0; i < 4; ++i) col_f.e[i] = (col_f.e[i] * f) * (float)PSY_INV_PI_D;
+	return col_f;
+}
+
+// GTRClosure::sample_pdf (:556-571).
+__device__ __forceinline__ float gtr_pdf(const Gtr& g, V3 in, V3 out, V3 n) {
+	V3 nn = normalized(n);
+	const V3 aa = normalized(in) * -1.0f;
+	const V3 bb = normalized(out);
+	const V3 hh = normalized((aa + bb) * 0.5f);
+	if (dot(nn, hh) < 0.0f) nn = nn * -1.0f;
+	const float nh = clampf(dot(nn, hh), -1.0f, 1.0f);
+	return gtr_dist(nh, g.rough, g.tail, g.norm) * (float)PSY_INV_PI_D;
+}
+
+// GTRClosure::sample (:428-449): a half vector from the distribution, the
+// mirror direction about it, its pdf and the closure's value.
+__device__ __forceinline__ void gtr_sample(const Gtr& g, V3 in, V3 n, float si, float sj, float wl, V3* out,
+                                           Spec* filter, float* pdf) {
+	V3 nn = normalized(n);
+	if (dot(nn, in) > 0.0f) nn = nn * -1.0f;
+	const float theta_cos = gtr_half_theta_sample(g, si);
+	const float theta_sin = sqrtf(1.0f - (theta_cos * theta_cos));
+	const float angle = (float)(((double)sj * PSY_PI_D) * 2.0);
+	V3 half_dir(cosf(angle) * theta_sin, sinf(angle) * theta_sin, theta_cos);
+	half_dir = normalized(zup_to_vec(half_dir, nn));
+	*out = in - ((half_dir * 2.0f) * dot(in, half_dir));
+	*pdf = gtr_pdf(g, in, *out, n);
+	*filter = gtr_eval(g, in, *out, n, wl);
+}
+
+// GTRClosure::estimate_eval_over_solid_angle (:519-553).
+__device__ __forceinline__ float gtr_estimate(const Gtr& g, V3 in, V3 cent, float cos_theta, V3 nor) {
+	V3 nn = normalized(nor);
+	const V3 aa = normalized(in) * -1.0f;
+	const V3 bb = normalized(cent);
+	if (dot(nn, in) > 0.0f) nn = nn * -1.0f;
+	const float theta = acosf(cos_theta);
+	const V3 hh = normalized(aa + bb);
+	const float nh = clampf(dot(nn, hh), -1.0f, 1.0f);
+	const float rough = smin(1.0f, sqrtf(g.rough) + ((2.0f * theta) / (float)PSY_PI_D));
+	const float fac = gtr_dist(nh, rough, g.tail, gtr_normalization(rough, g.tail));
+	return (fac * smin(1.0f - cos_theta, 1.0f)) * (float)PSY_INV_PI_D;
+}
+
+// Matrix44::setAxisAngle (math/matrix.hpp:345-372, after ImathMatrix.h) with
+// make_axis_angle_transform (math/transform.hpp:221-226).
+__device__ __forceinline__ M44 axis_angle(V3 axis, float angle) {
+	const V3 u = normalized(axis);
+	const float sine = sinf(angle), cosine = cosf(angle);
+	const float c1 = 1.0f - cosine;
+	M44 m;
+	m.m[0][0] = ((u.x * u.x) * c1) + cosine;
+	m.m[0][1] = ((u.x * u.y) * c1) + (u.z * sine);
+	m.m[0][2] = ((u.x * u.z) * c1) - (u.y * sine);
+	m.m[0][3] = 0.0f;
+	m.m[1][0] = ((u.x * u.y) * c1) - (u.z * sine);
+	m.m[1][1] = ((u.y * u.y) * c1) + cosine;
+	m.m[1][2] = ((u.y * u.z) * c1) + (u.x * sine);
+	m.m[1][3] = 0.0f;
+	m.m[2][0] = ((u.x * u.z) * c1) + (u.y * sine);
+	m.m[2][1] = ((u.y * u.z) * c1) - (u.x * sine);
+	m.m[2][2] = ((u.z * u.z) * c1) + cosine;
+	m.m[2][3] = 0.0f;
+	m.m[3][0] = 0.0f;
+	m.m[3][1] = 0.0f;
+	m.m[3][2] = 0.0f;
+	m.m[3][3] = 1.0f;
+	return m;
+}
+
+// reflect_ray_direction_differential and calc_uv_differentials
+// (basics/differential_geometry.hpp:113-156), clamp_dd (:125-135).
+__device__ __forceinline__ V3 reflect_dd(V3 normal, V3 normal_d, V3 d, V3 dd) {
+	const float ddn = dot(dd, normal) + dot(d, normal_d);
+	const V3 tmp = (normal_d * dot(d, normal)) + (normal * ddn);
+	return dd - (tmp * 2.0f);
+}
+__device__ __forceinline__ void uv_differentials(V3 dp, V3 dpdu, V3 dpdv, float* du, float* dv) {
+	const float dpdu_ilen = 1.0f / length(dpdu);
+	const V3 dpdu_n = dpdu * dpdu_ilen;
+	const float dpdv_ilen = 1.0f / length(dpdv);
+	const V3 dpdv_n = dpdv * dpdv_ilen;
+	*du = dot(dp, dpdu_n) * dpdu_ilen;
+	*dv = dot(dp, dpdv_n) * dpdv_ilen;
+}
+
+// ---------------------------------------------------------------------
 // Parameterised albedo (differentiable rendering; no reference counterpart)
 // ---------------------------------------------------------------------
 // Gaussian basis function k at wavelength w (nm).
@@ -381,6 +560,8 @@ struct LightQuery {
 	float n, u, v;
 	V3 pos, nor, d;
 	float wavelength, time;
+	bool gtr;             // the query's BSDF: GTR (gp) or Lambert
+	Gtr gp;
 	// out
 	M44 xform;
 	bool has_xform;
@@ -427,7 +608,7 @@ __device__ __forceinline__ float light_node_prob(const DevScene& sc, const Light
 		const float sin_theta_max2 = q2 < 1.0f ? q2 : 1.0f;
 		cos_theta_max = sqrtf(1.0f - sin_theta_max2);
 	}
-	const float est = lambert_estimate(q.d, d, cos_theta_max, q.nor);
+	const float est = q.gtr ? gtr_estimate(q.gp, q.d, d, cos_theta_max, q.nor) : lambert_estimate(q.d, d, cos_theta_max, q.nor);
 	const float approx_contrib = 0.0f < est ? est : 0.0f;
 	return nd.energy * inv_surface_area * approx_contrib;
 }

@@ -911,6 +911,21 @@ struct Builder {
 			ds.tail_shape = desc->shaders[s].tail_shape;
 			ds.fresnel = desc->shaders[s].fresnel;
 			if (ds.kind < 0 || ds.kind > 2) return fail("unknown shader kind");
+			if (ds.kind == SHADER_GTR) {
+				// GTRClosure::validate (shading/surface_closure.hpp:352-372)
+				float r = std::max(0.0f, std::min(0.9999f, ds.roughness));
+				float t = std::max(0.0001f, ds.tail_shape);
+				if (r < 0.000244140625f) r = 0.0f;
+				if (std::abs(t - 1.0f) < 0.0001f) t = 1.0f + 0.0001f;
+				ds.roughness = r;
+				ds.tail_shape = t;
+				// GTRClosure::normalization (:374-380)
+				const float r2 = r * r;
+				const float top = (t - 1.0f) * (r2 - 1);
+				const double bottom = M_PI * (double)(1.0f - std::pow(r2, 1.0f - t));
+				ds.norm = (float)((double)top / bottom);
+				ds.pow_r2_1mt = std::pow(r2, 1.0f - t);
+			}
 			out->shaders.push_back(ds);
 		}
 		// camera (basics/camera.hpp:28-64)

@@ -214,8 +214,10 @@ __device__ __forceinline__ void rect_light_at(const DevScene& sc, const DevObjec
 			*dx = a[0];
 			*dy = a[1];
 		} else {
-			*dx = lerp1(sp.nalpha, a[0], a[2]);
-			*dy = lerp1(sp.nalpha, a[1], a[3]);
+			// std::pair's operator* takes a float: (1 - alpha) is narrowed first
+			const float ia = one_minus(sp.nalpha);
+			*dx = (a[0] * ia) + (a[2] * sp.nalpha);
+			*dy = (a[1] * ia) + (a[3] * sp.nalpha);
 		}
 	}
 	if (col) {

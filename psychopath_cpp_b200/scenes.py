@@ -113,6 +113,35 @@ def adjoint_scene(seed: int = 1, res=(256, 256), spp: int = 32, n_spheres: int =
     return sc
 
 
+def gtr_scene(seed: int = 1, res=(96, 72), spp: int = 16, n_spheres: int = 24) -> Scene:
+    """The plain scene with GTR microfacet shaders (GTRClosure,
+    shading/surface_closure.hpp:339-608) on the ground and on most spheres:
+    roughness from mirror (0, a delta closure) to 0.8, tail shapes on both
+    sides of 1, Fresnel factors 0..1; the rest Lambert; one sphere light."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(name="gtr_%d" % seed, res_x=res[0], res_y=res[1], spp=spp, seed=1)
+    sc.camera = Camera(transforms=[look_at((0.0, -15.0, 7.0), (0.0, 0.0, 0.5))], fovs=[45.0])
+    root = sc.root
+    root.add_shader("ground_mat", SurfaceShader("GTR", [0.7, 0.65, 0.6], roughness=0.35, tail_shape=2.0, fresnel=0.5))
+    root.add_object("ground", BilinearPatch([[-10, -10, 0], [10, -10, 0], [-10, 10, 0], [10, 10, 0]]))
+    root.add_instance("ground", shader="ground_mat")
+    roughs = [0.0, 0.02, 0.1, 0.3, 0.6, 0.8]
+    for i in range(n_spheres):
+        col = [rng.uniform(0.2, 0.9), rng.uniform(0.2, 0.9), rng.uniform(0.2, 0.9)]
+        if i % 4 == 3:
+            root.add_shader("mat%d" % i, SurfaceShader("Lambert", col))
+        else:
+            root.add_shader("mat%d" % i, SurfaceShader("GTR", col, roughness=roughs[i % len(roughs)],
+                                                       tail_shape=[0.5, 1.0, 2.0, 4.0][i % 4],
+                                                       fresnel=rng.uniform(0.0, 1.0)))
+        root.add_object("sphere%d" % i, Sphere([rng.uniform(-5, 5), rng.uniform(-5, 5), rng.uniform(0, 2)],
+                                               rng.uniform(0.2, 0.6)))
+        root.add_instance("sphere%d" % i, shader="mat%d" % i)
+    root.add_object("light", SphereLight([[1.0, -1.0, 6.0]], [0.5], [[100.0] * 3]))
+    root.add_instance("light")
+    return sc
+
+
 def rect_light_scene(seed: int = 1, res=(96, 72), spp: int = 16, n_spheres: int = 24) -> Scene:
     """The plain scene's geometry lit by rectangle lights instead of a
     sphere light: one overhead (3 x 1.5, facing down through an instance

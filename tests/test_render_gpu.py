@@ -150,3 +150,16 @@ def test_rect_light_sample_parity(ctx, ref_available):
     for name, sl in (("to_light", slice(0, 3)), ("spec", slice(3, 7)), ("light_pdf", slice(9, 10))):
         d = parity.ulp_diff(ref_out[same, sl], out[same, sl])
         assert np.percentile(d, 99) <= 8, (name, np.percentile(d, 99), int(d.max()))
+
+
+def test_gtr_render(ctx, ref_available):
+    """GTR microfacet closures (shading/surface_closure.hpp:339-608):
+    sampling, evaluation, pdf and MIS, the light tree's GTR estimate, the
+    GTR ray-differential transport, and a mirror (delta) closure."""
+    sc = scenes.gtr_scene(1, res=(96, 72), spp=16)
+    (rx, rc, rrays), (mx, mc, mrays) = _render_both(ctx, sc, 16, 4)
+    assert (rc == mc).all()
+    err, npx = rel_rmse(mx, rx)
+    assert npx > 3000
+    assert err <= IMAGE_REL_RMSE, err
+    assert abs(int(rrays) - int(mrays)) <= 0.001 * rrays, (rrays, mrays)
