@@ -49,15 +49,20 @@ def _light_queries(n, lo, hi, seed):
     return q
 
 
-@pytest.mark.parametrize("which", ["plain", "many"])
+@pytest.mark.parametrize("which", ["plain", "many", "bench"])
 def test_light_tree_sample_parity(ctx, ref_available, which):
+    """LightTree::sample; "bench" is the 720p benchmark scene's own tree
+    (10,000 sphere lights, 19,999 nodes) with queries over its ground."""
     from oracle import psyref
     if which == "plain":
         sc = scenes.plain_scene(4)
         q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 3), 1)
-    else:
+    elif which == "many":
         sc = scenes.many_light_scene(6, res=(64, 36), spp=1, n_patches=60, n_groups=30, n_lights=2000)
         q = _light_queries(20000, (-8, -6, 0.0), (8, 6, 4), 2)
+    else:
+        sc = scenes.many_light_scene(3, res=(64, 36), spp=1)
+        q = _light_queries(50000, (-24, -19, 0.0), (24, 19, 2), 5)
     ref_out, ref_ids = psyref.RefScene(scene=sc).light_sample(q)
     ctx.upload(sc)
     out, ids = api.LightTree(ctx).sample(q)
