@@ -75,8 +75,9 @@ __device__ __forceinline__ LocalRay make_local_x(const WorldRayD& wr, const M44&
 }
 
 // The width parameters update_ray computes beside the local ray `r` (made
-// from wr with transform t, or none).
-__device__ __forceinline__ RayWidth ray_width_of(const WorldRayD& wr, const LocalRay& r, const M44* t) {
+// from wr with transform t, or none).  Computed once per space a ray meets
+// a patch in, so it is not inlined (smaller traversal code).
+__device__ __noinline__ RayWidth ray_width_of(const WorldRayD& wr, const LocalRay& r, const M44* t) {
 	if (!t) return ray_width_params(r.o, r.d, wr.odx, wr.ody, wr.ddx, wr.ddy);
 	return ray_width_params(r.o, r.d, dir_to(*t, wr.odx), dir_to(*t, wr.ody), dir_to(*t, wr.ddx), dir_to(*t, wr.ddy));
 }
@@ -101,31 +102,33 @@ __device__ __forceinline__ M44 seq_lerp_global(const float* xs, int count, float
 
 // merge() of transform sequences (math/transform.hpp:241-272): parent `a`
 // with instance transforms `b` (global, count nb), written into `dst`.
-// Returns false if the result needs more than PSY_MAX_MOTION samples.
-__device__ __forceinline__ bool frame_merge(const Frame& a, const float* b, int nb, Frame* dst) {
+// Returns false if the result needs more than PSY_MAX_MOTION samples.  The
+// three cases of the reference (equal counts, more parent samples, more
+// instance samples) share one loop with one matrix product, and the function
+// is not inlined: its callers run it rarely (entering a transformed
+// instance), and one copy of the code keeps the traversal kernels' code
+// small enough for the instruction cache.
+__device__ __noinline__ bool frame_merge(const Frame& a, const float* b, int nb, Frame* dst) {
 	const int na = a.count;
 	if (na > PSY_MAX_MOTION || nb > PSY_MAX_MOTION) return false;
-	if (na == nb) {
-		for (int i = 0; i < na; ++i) dst->m[i] = m44_mul(a.m[i], load_m44_dev(b + 16 * i));
-		dst->count = na;
-	} else if (na > nb) {
-		if (nb == 0) {
-			for (int i = 0; i < na; ++i) dst->m[i] = a.m[i];
+	const int n = na > nb ? na : nb;
+	const float inv_s = n > 1 ? 1.0f / (float)(n - 1) : 0.0f;
+#pragma unroll 1
+	for (int i = 0; i < n; ++i) {
+		M44 r;
+		if (na == nb) {
+			r = m44_mul(a.m[i], load_m44_dev(b + 16 * i));
+		} else if (na > nb) {
+			if (nb == 0) r = a.m[i];
+			else r = m44_mul(a.m[i], seq_lerp_global(b, nb, (float)i * inv_s));
 		} else {
-			const float inv_s = 1.0f / (float)(na - 1);
-			for (int i = 0; i < na; ++i) dst->m[i] = m44_mul(a.m[i], seq_lerp_global(b, nb, (float)i * inv_s));
+			// the reference multiplies instance * lerped-parent in this case
+			if (na == 0) r = load_m44_dev(b + 16 * i);
+			else r = m44_mul(load_m44_dev(b + 16 * i), frame_at_index_lerp(a, (float)i * inv_s));
 		}
-		dst->count = na;
-	} else {
-		if (na == 0) {
-			for (int i = 0; i < nb; ++i) dst->m[i] = load_m44_dev(b + 16 * i);
-		} else {
-			const float inv_s = 1.0f / (float)(nb - 1);
-			// The reference multiplies instance * lerped-parent in this branch.
-			for (int i = 0; i < nb; ++i) dst->m[i] = m44_mul(load_m44_dev(b + 16 * i), frame_at_index_lerp(a, (float)i * inv_s));
-		}
-		dst->count = nb;
+		dst->m[i] = r;
 	}
+	dst->count = n;
 	return true;
 }
 
@@ -1138,9 +1141,10 @@ __device__ __forceinline__ void leave_levels(TraceState<F>& s) {
 // Enters the assembly of instance `inst` (global index gi, element id
 // `id`, inherited shader): merges its transforms into the level's frame,
 // moves the ray into its space and pushes its root.  Returns false when the
-// node stack overflows.
+// node stack overflows.  Not inlined: a ray enters few instances, and one
+// copy keeps the traversal kernels' code small.
 template <unsigned F>
-__device__ __forceinline__ bool enter_assembly(const DevScene& sc, TraceState<F>& s, const DevInstance& inst, int gi,
+__device__ __noinline__ bool enter_assembly(const DevScene& sc, TraceState<F>& s, const DevInstance& inst, int gi,
                                                uint64_t id, int shader) {
 	constexpr bool XFORM = (F & FEAT_XFORM) != 0;
 	const WorldRayD& wr = s.wr;
