@@ -77,7 +77,7 @@ __device__ __forceinline__ LocalRay make_local_x(const WorldRayD& wr, const M44&
 // The width parameters update_ray computes beside the local ray `r` (made
 // from wr with transform t, or none).  Computed once per space a ray meets
 // a patch in, so it is not inlined (smaller traversal code).
-__device__ __noinline__ RayWidth ray_width_of(const WorldRayD& wr, const LocalRay& r, const M44* t) {
+static __device__ __noinline__ RayWidth ray_width_of(const WorldRayD& wr, const LocalRay& r, const M44* t) {
 	if (!t) return ray_width_params(r.o, r.d, wr.odx, wr.ody, wr.ddx, wr.ddy);
 	return ray_width_params(r.o, r.d, dir_to(*t, wr.odx), dir_to(*t, wr.ody), dir_to(*t, wr.ddx), dir_to(*t, wr.ddy));
 }
@@ -108,7 +108,7 @@ __device__ __forceinline__ M44 seq_lerp_global(const float* xs, int count, float
 // is not inlined: its callers run it rarely (entering a transformed
 // instance), and one copy of the code keeps the traversal kernels' code
 // small enough for the instruction cache.
-__device__ __noinline__ bool frame_merge(const Frame& a, const float* b, int nb, Frame* dst) {
+static __device__ __noinline__ bool frame_merge(const Frame& a, const float* b, int nb, Frame* dst) {
 	const int na = a.count;
 	if (na > PSY_MAX_MOTION || nb > PSY_MAX_MOTION) return false;
 	const int n = na > nb ? na : nb;
