@@ -185,7 +185,7 @@ __device__ void make_stored(const DevScene& sc, const HitRec& rec, const WorldRa
 	if (h.closure != CLOSURE_LAMBERT && h.closure != CLOSURE_GTR) return;
 	M44 inv;
 	if (xf) {
-		inv = m44_inverse(space, sc.rcp);
+		inv = m44_inverse_dev(space, sc.rcp);
 	} else {
 		inv = m44_identity();
 		for (int i = 0; i < 4; ++i) inv.m[i][i] = ident_inv;
@@ -235,7 +235,7 @@ __device__ __forceinline__ void propagate_differentials(const StoredHit& h, Worl
 // origin differentials transferred to the hit, normal differentials turned
 // into half-vector differentials, direction differentials reflected about
 // the half vector, then clamped (clamp_dd).
-__device__ void gtr_propagate_differentials(const StoredHit& h, WorldRayD* out) {
+static __device__ __noinline__ void gtr_propagate_differentials(const StoredHit& h, WorldRayD* out) {
 	V3 nn = normalized(h.n);
 	const V3 hh = normalized(normalized(h.d * -1.0f) + normalized(out->d));
 	out->odx = transfer_origin_differential(h.t, nn, h.d, h.odx, h.ddx);

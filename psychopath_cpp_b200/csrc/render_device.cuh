@@ -278,7 +278,9 @@ static __device__ float spectrum_xyz_to_p(float lambda, const float* xyz) {
 }
 
 // Color_to_XYZ (color/color.hpp:476-487) then XYZ_to_SpectralSample.
-__device__ __forceinline__ Spec rgb_to_spec(const float* col, float hero) {
+// Not inlined: called several times per path step, one copy of its code
+// keeps the shading kernels small.
+static __device__ __noinline__ Spec rgb_to_spec(const float* col, float hero) {
 	float xyz[3];
 	xyz[0] = (col[0] * 0.4339f) + (col[1] * 0.3762f) + (col[2] * 0.1899f);
 	xyz[1] = (col[0] * 0.2126f) + (col[1] * 0.7152f) + (col[2] * 0.0722f);
@@ -386,7 +388,7 @@ __device__ __forceinline__ float schlick_fresnel_from_fac(float f, float c) {
 }
 
 // GTRClosure::evaluate (:452-516).
-__device__ __forceinline__ Spec gtr_eval(const Gtr& g, V3 in, V3 out, V3 n, float wl) {
+static __device__ __noinline__ Spec gtr_eval(const Gtr& g, V3 in, V3 out, V3 n, float wl) {
 	V3 nn = normalized(n);
 	const V3 aa = normalized(in) * -1.0f;
 	const V3 bb = normalized(out);
@@ -424,7 +426,7 @@ __device__ __forceinline__ Spec gtr_eval(const Gtr& g, V3 in, V3 out, V3 n, floa
 }
 
 // GTRClosure::sample_pdf (:556-571).
-__device__ __forceinline__ float gtr_pdf(const Gtr& g, V3 in, V3 out, V3 n) {
+static __device__ __noinline__ float gtr_pdf(const Gtr& g, V3 in, V3 out, V3 n) {
 	V3 nn = normalized(n);
 	const V3 aa = normalized(in) * -1.0f;
 	const V3 bb = normalized(out);
@@ -436,7 +438,7 @@ __device__ __forceinline__ float gtr_pdf(const Gtr& g, V3 in, V3 out, V3 n) {
 
 // GTRClosure::sample (:428-449): a half vector from the distribution, the
 // mirror direction about it, its pdf and the closure's value.
-__device__ __forceinline__ void gtr_sample(const Gtr& g, V3 in, V3 n, float si, float sj, float wl, V3* out,
+static __device__ __noinline__ void gtr_sample(const Gtr& g, V3 in, V3 n, float si, float sj, float wl, V3* out,
                                            Spec* filter, float* pdf) {
 	V3 nn = normalized(n);
 	if (dot(nn, in) > 0.0f) nn = nn * -1.0f;
@@ -451,7 +453,7 @@ __device__ __forceinline__ void gtr_sample(const Gtr& g, V3 in, V3 n, float si, 
 }
 
 // GTRClosure::estimate_eval_over_solid_angle (:519-553).
-__device__ __forceinline__ float gtr_estimate(const Gtr& g, V3 in, V3 cent, float cos_theta, V3 nor) {
+static __device__ __noinline__ float gtr_estimate(const Gtr& g, V3 in, V3 cent, float cos_theta, V3 nor) {
 	V3 nn = normalized(nor);
 	const V3 aa = normalized(in) * -1.0f;
 	const V3 bb = normalized(cent);
@@ -592,7 +594,7 @@ __device__ __forceinline__ Box light_node_box(const DevScene& sc, const DevLight
 	return box_lerp(sp.nalpha, sample(sp.i0), sample(sp.i0 + 1));
 }
 
-__device__ __forceinline__ float light_node_prob(const DevScene& sc, const LightQuery& q, int index) {
+static __device__ __noinline__ float light_node_prob(const DevScene& sc, const LightQuery& q, int index) {
 	const DevLightNode nd = sc.light_nodes[index];
 	const Box bbox = light_node_box(sc, nd, q.time);
 	const V3 d = box_center(bbox) - q.pos;
@@ -614,7 +616,7 @@ __device__ __forceinline__ float light_node_prob(const DevScene& sc, const Light
 }
 
 // SphereLight::sample; returns the colour scale and writes the shadow vector and pdf.
-static __device__ void sphere_light_sample(const DevScene& sc, const DevObject& ob, V3 arr, float u, float v, float wl,
+static __device__ __noinline__ void sphere_light_sample(const DevScene& sc, const DevObject& ob, V3 arr, float u, float v, float wl,
                                     float time, V3* shadow_vec, float* pdf, Spec* spec) {
 	V3 pos;
 	float radius_f;
@@ -672,7 +674,7 @@ static __device__ void sphere_light_sample(const DevScene& sc, const DevObject& 
 // Arvo, "Stratified Sampling of Spherical Triangles", 1995): the angles in
 // double as there; the vector arithmetic is Vec3's float arithmetic, each
 // double factor rounded to float where it scales a Vec3.
-static __device__ V3 uniform_sample_spherical_triangle(V3 A, V3 B, V3 C, float i, float j) {
+static __device__ __noinline__ V3 uniform_sample_spherical_triangle(V3 A, V3 B, V3 C, float i, float j) {
 	auto clampd = [](double v) { return fmin(1.0, fmax(-1.0, v)); };
 	const double cos_a = clampd((double)dot(B, C));
 	const double cos_b = clampd((double)dot(C, A));
@@ -705,7 +707,7 @@ static __device__ V3 uniform_sample_spherical_triangle(V3 A, V3 B, V3 C, float i
 // RectangleLight::sample (lights/rectangle_light.hpp:40-71): one of the
 // rectangle's two spherical triangles, chosen by solid angle, sampled
 // uniformly and projected back onto the rectangle.
-static __device__ void rect_light_sample(const DevScene& sc, const DevObject& ob, V3 arr, float u, float v, float wl,
+static __device__ __noinline__ void rect_light_sample(const DevScene& sc, const DevObject& ob, V3 arr, float u, float v, float wl,
                                          float time, V3* shadow_vec, float* pdf, Spec* spec) {
 	float dx, dy, col[3];
 	rect_light_at(sc, ob, time, &dx, &dy, col);
@@ -725,6 +727,11 @@ static __device__ void rect_light_sample(const DevScene& sc, const DevObject& ob
 	const float c[3] = {(col[0] * isa) * 0.5f, (col[1] * isa) * 0.5f, (col[2] * isa) * 0.5f};
 	*spec = rgb_to_spec(c, wl);
 }
+
+// Matrix44::inverse on the device, not inlined: only transformed hits and
+// instanced lights need it, and one copy keeps the shading kernels' code
+// small.
+static __device__ __noinline__ M44 m44_inverse_dev(const M44& a, const RcpTable& rt) { return m44_inverse(a, rt); }
 
 // LightTree::sample starting at the root assembly's tree.
 static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, float ident_inv) {
@@ -766,7 +773,7 @@ static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, floa
 		if (inst.xform_count > 0) {
 			const M44 X = seq_lerp_global(sc.xforms + (size_t)inst.xform * 16, inst.xform_count, q->time);
 			q->pos = pos_to(X, q->pos);
-			q->nor = normalized(nor_to(X, q->nor, sc.rcp));
+			q->nor = normalized(dir_transpose(m44_inverse_dev(X, sc.rcp), q->nor));
 			q->xform = q->has_xform ? m44_mul(q->xform, X) : m44_mul(m44_identity(), X);
 			q->has_xform = true;
 		}
@@ -782,7 +789,7 @@ static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, floa
 				rect_light_sample(sc, ob, q->pos, q->u, q->v, q->wavelength, q->time, &tl, &p, &q->spec);
 			// xform.dir_from: the reference inverts the accumulated transform,
 			// which is the identity when no instance carried one
-			if (q->has_xform) q->to_light = dir_from(q->xform, tl, sc.rcp);
+			if (q->has_xform) q->to_light = dir_to(m44_inverse_dev(q->xform, sc.rcp), tl);
 			else q->to_light = tl * ident_inv;
 			q->selection_pdf *= (tot_prob * (float)as.light_count);
 			q->light_sample_pdf = p;
