@@ -215,14 +215,14 @@ def test_device_built_bvh_gives_the_same_hits(ctx, ref_available, kind):
         rep = parity.compare_trace(ref, mine, rays["type"])
         parity.assert_parity(rep)
     assert (host_tree["hit"] == dev_tree["hit"]).all()
-    # a device-built tree renders the same image as the host-built one, up to exact ties
-    from psychopath_cpp_b200 import api as A
+    # a device-built tree renders the same image as the host-built one, up to
+    # exact ties between candidates (met in another order)
     ctx.upload(sc)
-    a, _ = A.PathTraceIntegrator(ctx, 64, 48, 4, seed=1, path_length=4).integrate()
+    a, _ = api.PathTraceIntegrator(ctx, 64, 48, 4, seed=1, path_length=4).integrate()
     ctx.upload(sc, gpu_bvh=True)
-    b, _ = A.PathTraceIntegrator(ctx, 64, 48, 4, seed=1, path_length=4).integrate()
-    m = a[..., 1] > 0
-    assert np.abs(a[..., 1][m] - b[..., 1][m]).max() <= 1e-5 * a[..., 1].max()
+    b, _ = api.PathTraceIntegrator(ctx, 64, 48, 4, seed=1, path_length=4).integrate()
+    m = a[..., 1] > 1e-6 * a[..., 1].max()
+    assert (a[..., 1][m] == b[..., 1][m]).mean() > 0.999
 
 
 def test_rect_light_hits(ctx, ref_available):
