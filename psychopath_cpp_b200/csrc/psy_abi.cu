@@ -98,6 +98,8 @@ int psy_ctx::check_status(cudaStream_t stream) {
 			return ctx_fail(this, PSY_ERR_STACK_OVERFLOW, "assembly nesting deeper than supported (flags %#x)", st);
 		if (st & ERRF_MOTION)
 			return ctx_fail(this, PSY_ERR_ARG, "more motion samples than supported (flags %#x)", st);
+		if (st & ERRF_BISECT)
+			return ctx_fail(this, PSY_ERR_TIMEOUT, "a patch bisection exceeded its step bound (flags %#x)", st);
 		return ctx_fail(this, PSY_ERR_DEVICE, "device error flags %#x", st);
 	}
 	return PSY_OK;

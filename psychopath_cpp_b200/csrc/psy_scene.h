@@ -29,7 +29,8 @@ enum : int { SHADER_LAMBERT = 0, SHADER_EMIT = 1, SHADER_GTR = 2 };
 enum : int { CLOSURE_NONE = 0, CLOSURE_LAMBERT = 1, CLOSURE_EMIT = 2, CLOSURE_GTR = 3 };
 
 // Device error flags, OR-ed into the context's status word by kernels.
-enum : unsigned { ERRF_STACK = 1u, ERRF_LEVELS = 2u, ERRF_MOTION = 4u, ERRF_TIMEOUT = 8u, ERRF_NOLIGHT = 16u };
+enum : unsigned { ERRF_STACK = 1u, ERRF_LEVELS = 2u, ERRF_MOTION = 4u, ERRF_TIMEOUT = 8u, ERRF_NOLIGHT = 16u,
+                  ERRF_BISECT = 32u /* a patch bisection exceeded its step bound */ };
 
 // Scene features that select a compiled variant of the traversal kernels.
 enum : unsigned {

@@ -503,7 +503,14 @@ struct PatchCursor {
 	Bits128 gpend;
 	unsigned gmask;
 	bool act, fresh;
+	unsigned steps;  // group steps taken (bounded: PSY_PATCH_MAX_STEPS)
 };
+
+// A bisection ends with an error after this many group steps.  The walk is
+// finite (a leaf is forced at 63 second halves or depth 127), but a ray the
+// reference would bisect for hours must not hold a wave: far above any
+// bisection of a real scene.
+#define PSY_PATCH_MAX_STEPS (1u << 24)
 
 // Sub-patches stored on the current path (with their uv ranges).
 template <int NV, int TSC>
@@ -757,7 +764,7 @@ template <int NV, int TSC>
 __device__ __forceinline__ bool patch_units_warp(PatchCursor<NV, TSC>& pc, PatchStore<NV, TSC>& ps,
                                                  const float* verts, const LocalRay& r, const RayWidth& rw,
                                                  float* max_t, bool occl, float dice_rate, float min_upoly,
-                                                 PatchHit* hit, bool in, int& units) {
+                                                 PatchHit* hit, bool in, int& units, unsigned* err) {
 	constexpr unsigned FULL = 0xffffffffu;
 	const unsigned lane = threadIdx.x & 31u;
 	const bool start = in && pc.fresh;
@@ -769,6 +776,7 @@ __device__ __forceinline__ bool patch_units_warp(PatchCursor<NV, TSC>& pc, Patch
 		pc.fresh = false;
 		pc.gpend = Bits128{0, 0};
 		pc.act = true;
+		pc.steps = 0;
 	}
 	bool done = false;
 	for (int u = 0; u < units; ++u) {
@@ -778,6 +786,14 @@ __device__ __forceinline__ bool patch_units_warp(PatchCursor<NV, TSC>& pc, Patch
 		}
 		// leaf test of the lanes whose ray hits the node
 		bool fin = false;
+		if (in && ++pc.steps > PSY_PATCH_MAX_STEPS) {
+			// give up on this ray's bisection: the caller reports ERRF_BISECT
+			fin = true;
+			pc.act = false;
+			pc.pend = Bits128{0, 0};
+			pc.found = false;
+			*err |= ERRF_BISECT;
+		}
 		if (in && pc.act) {
 			const float wm = ray_min_width(rw, pc.h0, pc.h1) * dice_rate;
 			const float width = (wm != wm) ? min_upoly : smax(wm, min_upoly);
@@ -842,6 +858,9 @@ __device__ __forceinline__ bool patch_units_warp(PatchCursor<NV, TSC>& pc, Patch
 				pc.h0 = fh0;
 				pc.h1 = fh1;
 			} else {
+				// no lane's ray hits either half: the node is done for every
+				// lane of the group
+				pc.act = false;
 				resume = true;
 			}
 			if (any_s || any_f) {
@@ -1435,7 +1454,8 @@ __device__ __forceinline__ bool patch_step_warp(const DevScene& sc, TraceState<F
 		typename std::remove_reference<decltype(pw.c)>::type pc;
 		if (in_m) pc = pw.c;
 		int left = units;
-		const bool d = patch_units_warp(pc, pw.st, s.pverts, s.pr, s.prw, &max_t, occl, dr, mu, &s.ph, in_m, left);
+		const bool d = patch_units_warp(pc, pw.st, s.pverts, s.pr, s.prw, &max_t, occl, dr, mu, &s.ph, in_m, left,
+		                                &s.err);
 		if (in_m) {
 			done = d;
 			found = pc.found;
