@@ -349,6 +349,21 @@ int psy_film_srgb8(psy_ctx* ctx, const float* xyz, const uint32_t* counts, uint3
                    int dithered, uint32_t seed, uint8_t* rgb, void* stream);
 
 /*
+ * Self-check of the device float math (no counterpart in the reference).
+ * The shading kernels evaluate sin, cos, acos, asin and exp of floats with
+ * restatements of the host C library's sincosf, acosf, asinf and expf, so
+ * their bits follow the reference's std::sin/cos/acos/asin/exp calls.
+ * psy_math_check evaluates function `fn` on the device for the n host
+ * floats x into the n host floats out (synchronous).
+ */
+#define PSY_MATH_SIN 0u
+#define PSY_MATH_COS 1u
+#define PSY_MATH_ACOS 2u
+#define PSY_MATH_ASIN 3u
+#define PSY_MATH_EXP 4u
+int psy_math_check(psy_ctx* ctx, uint32_t fn, uint32_t n, const float* x, float* out);
+
+/*
  * Optional timing of the traversal kernels, for roofline reports (no
  * counterpart in the reference).  While enabled, psy_render records CUDA
  * events on its stream around every traversal launch (the event pool starts

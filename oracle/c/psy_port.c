@@ -468,3 +468,25 @@ int psyport_box_hit(const float* lo, const float* hi, const float* o, const floa
 uint64_t psyport_id_push(uint64_t id, uint64_t sub, int bits) {
 	return (id << bits) | (sub & (uint64_t)(int64_t)((1 << bits) - 1));
 }
+
+/*
+ * The host C library's float math as the reference calls it (std::sin and
+ * std::cos of one float become sincosf under GCC; std::acos, std::asin and
+ * std::exp of a float become acosf, asinf and expf), evaluated over an
+ * array: fn 0 sin, 1 cos, 2 acos, 3 asin, 4 exp.
+ */
+void sincosf(float x, float* s, float* c);
+int psyport_libm(int fn, uint32_t n, const float* x, float* out) {
+	for (uint32_t i = 0; i < n; ++i) {
+		float s, c;
+		switch (fn) {
+			case 0: sincosf(x[i], &s, &c); out[i] = s; break;
+			case 1: sincosf(x[i], &s, &c); out[i] = c; break;
+			case 2: out[i] = acosf(x[i]); break;
+			case 3: out[i] = asinf(x[i]); break;
+			case 4: out[i] = expf(x[i]); break;
+			default: return -1;
+		}
+	}
+	return 0;
+}

@@ -32,6 +32,8 @@ def lib():
         L.psyport_id_push.restype = C.c_uint64
         L.psyport_trace.argtypes = [C.POINTER(_abi.SceneDesc), C.POINTER(_abi.RaySoA), C.c_uint32, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p]
+        L.psyport_libm.argtypes = [C.c_int, C.c_uint32, fp, fp]
+        L.psyport_libm.restype = C.c_int
         _lib = L
     return _lib
 
@@ -65,3 +67,17 @@ def box_hit(lo, hi, o, d, tmax=float("inf")):
 
 def id_push(idv: int, sub: int, bits: int) -> int:
     return int(lib().psyport_id_push(idv, sub, bits))
+
+
+LIBM_FUNCTIONS = ("sin", "cos", "acos", "asin", "exp")
+
+
+def libm(fn: str, x: np.ndarray) -> np.ndarray:
+    """The host C library's float `fn` (sincosf / acosf / asinf / expf, as
+    the reference's std:: calls of a float resolve) of every element."""
+    x = np.ascontiguousarray(x, np.float32).ravel()
+    out = np.empty_like(x)
+    fp = C.POINTER(C.c_float)
+    rc = lib().psyport_libm(LIBM_FUNCTIONS.index(fn), x.size, x.ctypes.data_as(fp), out.ctypes.data_as(fp))
+    assert rc == 0
+    return out

@@ -146,7 +146,7 @@ EXPORTED = ["psy_ctx_create", "psy_ctx_destroy", "psy_last_error", "psy_version"
             "psy_scene_stats_get", "psy_build_bvh4", "psy_build_light_tree", "psy_trace", "psy_trace_host", "psy_sync",
             "psy_trace_host_noalloc", "psy_render_batch", "psy_batch_autotune", "psy_render_diff",
             "psy_render_adjoint", "psy_profile_enable", "psy_profile_read", "psy_profile_counters",
-            "psy_light_sample", "psy_render", "psy_film_srgb8"]
+            "psy_light_sample", "psy_render", "psy_film_srgb8", "psy_math_check"]
 
 _lib = None
 
@@ -192,6 +192,8 @@ def load():
     if hasattr(L, "psy_light_sample"):
         L.psy_light_sample.argtypes = [C.c_void_p, C.POINTER(LightQuerySoA), C.c_uint32,
                                        C.POINTER(LightSampleSoA), C.c_void_p]
+    if hasattr(L, "psy_math_check"):
+        L.psy_math_check.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, fp, fp]
     if hasattr(L, "psy_film_srgb8"):
         L.psy_film_srgb8.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32,
                                      C.c_void_p, C.c_void_p]

@@ -200,6 +200,19 @@ class Context:
         self.check(self.L.psy_profile_counters(self.h, C.byref(c), C.byref(o)))
         return {"closest": c.as_dict(), "occlusion": o.as_dict()}
 
+    MATH_FUNCTIONS = ("sin", "cos", "acos", "asin", "exp")
+
+    def math_check(self, fn: str, x: np.ndarray) -> np.ndarray:
+        """The device's float `fn` (one of MATH_FUNCTIONS) of every element
+        of `x` (psy_math_check): the restatements of the host C library's
+        sincosf / acosf / asinf / expf that the shading kernels use."""
+        x = np.ascontiguousarray(x, np.float32).ravel()
+        out = np.empty_like(x)
+        fp = C.POINTER(C.c_float)
+        self.check(self.L.psy_math_check(self.h, self.MATH_FUNCTIONS.index(fn), x.size, x.ctypes.data_as(fp),
+                                         out.ctypes.data_as(fp)))
+        return out
+
 
 def _check(L, rc: int, what: str):
     if rc != 0:

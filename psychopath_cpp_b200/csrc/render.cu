@@ -251,7 +251,7 @@ static __device__ __noinline__ void gtr_propagate_differentials(const StoredHit&
 		dndy = dndy * -1.0f;
 	}
 	const V3 axis = normalized(cross(nn, hh));
-	const float angle = acosf(clampf(dot(nn, hh), 0.0f, 1.0f));
+	const float angle = lm_acosf(clampf(dot(nn, hh), 0.0f, 1.0f));
 	const M44 xf = axis_angle(axis, angle);
 	const V3 dhdx = dir_to(xf, dndx);
 	const V3 dhdy = dir_to(xf, dndy);

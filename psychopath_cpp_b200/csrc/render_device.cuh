@@ -17,6 +17,7 @@
 
 #include "kernels.h"
 #include "shade_geom.cuh"
+#include "psy_libm.cuh"
 
 #define PSY_SPEC_QUAL __device__
 #include "spectral_table.inc"
@@ -120,8 +121,10 @@ __device__ __forceinline__ void square_to_circle(float* x, float* y) {
 		radius = -*y;
 		angle = (float)(PSY_QPI_D * (double)(6.0f - (*x / *y)));
 	}
-	*x = radius * cosf(angle);
-	*y = radius * sinf(angle);
+	float sine, cosine;
+	lm_sincosf(angle, &sine, &cosine);
+	*x = radius * cosine;
+	*y = radius * sine;
 }
 
 __device__ __forceinline__ V3 cosine_sample_hemisphere(float u, float v) {
@@ -156,7 +159,9 @@ __device__ __forceinline__ V3 uniform_sample_sphere(float u, float v) {
 	const float t = 1.f - z * z;
 	const float r = sqrtf(0.f < t ? t : 0.f);
 	const float phi = (float)((2.0 * PSY_PI_D) * (double)v);
-	return V3(r * cosf(phi), r * sinf(phi), z);
+	float sine, cosine;
+	lm_sincosf(phi, &sine, &cosine);
+	return V3(r * cosine, r * sine, z);
 }
 
 // sphere_lambert (utils/monte_carlo.hpp:207-233).
@@ -168,10 +173,10 @@ __device__ __forceinline__ float sphere_lambert(float nlcos, float rcos) {
 	const float ycos2 = (float)(1.0 - (double)(ysin * ysin));
 	const float ycos = sqrtf(ycos2);
 	const float g = (float)(((((-2.0 * (double)nlsin) * (double)rcos) * (double)ycos) + PSY_HPI_D) -
-	                        (double)asinf(ysin) + (double)(ysin * ycos));
-	const float h = nlcos * ((ycos * sqrtf(rsin2 - ycos2)) + (rsin2 * asinf(ycos / rsin)));
-	const float nl = acosf(nlcos);
-	const float r = acosf(rcos);
+	                        (double)lm_asinf(ysin) + (double)(ysin * ycos));
+	const float h = nlcos * ((ycos * sqrtf(rsin2 - ycos2)) + (rsin2 * lm_asinf(ycos / rsin)));
+	const float nl = lm_acosf(nlcos);
+	const float r = lm_acosf(rcos);
 	if ((double)nl < (PSY_HPI_D - (double)r)) return nlcos * rsin2;
 	if ((double)nl < PSY_HPI_D) return (nlcos * rsin2) + g - h;
 	if ((double)nl < (PSY_HPI_D + (double)r)) return (float)((double)(g + h) * PSY_INV_PI_D);
@@ -201,17 +206,17 @@ __device__ __forceinline__ float X_1931(float w) {
 	const float t1 = (w - 442.0f) * ((w < 442.0f) ? 0.0624f : 0.0374f);
 	const float t2 = (w - 599.8f) * ((w < 599.8f) ? 0.0264f : 0.0323f);
 	const float t3 = (w - 501.1f) * ((w < 501.1f) ? 0.0490f : 0.0382f);
-	return (0.362f * expf(-0.5f * t1 * t1)) + (1.056f * expf(-0.5f * t2 * t2)) - (0.065f * expf(-0.5f * t3 * t3));
+	return (0.362f * lm_expf(-0.5f * t1 * t1)) + (1.056f * lm_expf(-0.5f * t2 * t2)) - (0.065f * lm_expf(-0.5f * t3 * t3));
 }
 __device__ __forceinline__ float Y_1931(float w) {
 	const float t1 = (w - 568.8f) * ((w < 568.8f) ? 0.0213f : 0.0247f);
 	const float t2 = (w - 530.9f) * ((w < 530.9f) ? 0.0613f : 0.0322f);
-	return (0.821f * expf(-0.5f * t1 * t1)) + (0.286f * expf(-0.5f * t2 * t2));
+	return (0.821f * lm_expf(-0.5f * t1 * t1)) + (0.286f * lm_expf(-0.5f * t2 * t2));
 }
 __device__ __forceinline__ float Z_1931(float w) {
 	const float t1 = (w - 437.0f) * ((w < 437.0f) ? 0.0845f : 0.0278f);
 	const float t2 = (w - 459.0f) * ((w < 459.0f) ? 0.0385f : 0.0725f);
-	return (1.217f * expf(-0.5f * t1 * t1)) + (0.681f * expf(-0.5f * t2 * t2));
+	return (1.217f * lm_expf(-0.5f * t1 * t1)) + (0.681f * lm_expf(-0.5f * t2 * t2));
 }
 
 // spectrum_xyz_to_p (color/spectrum_grid.h:21-135).
@@ -445,7 +450,9 @@ static __device__ __noinline__ void gtr_sample(const Gtr& g, V3 in, V3 n, float 
 	const float theta_cos = gtr_half_theta_sample(g, si);
 	const float theta_sin = sqrtf(1.0f - (theta_cos * theta_cos));
 	const float angle = (float)(((double)sj * PSY_PI_D) * 2.0);
-	V3 half_dir(cosf(angle) * theta_sin, sinf(angle) * theta_sin, theta_cos);
+	float sine, cosine;
+	lm_sincosf(angle, &sine, &cosine);
+	V3 half_dir(cosine * theta_sin, sine * theta_sin, theta_cos);
 	half_dir = normalized(zup_to_vec(half_dir, nn));
 	*out = in - ((half_dir * 2.0f) * dot(in, half_dir));
 	*pdf = gtr_pdf(g, in, *out, n);
@@ -458,7 +465,7 @@ static __device__ __noinline__ float gtr_estimate(const Gtr& g, V3 in, V3 cent, 
 	const V3 aa = normalized(in) * -1.0f;
 	const V3 bb = normalized(cent);
 	if (dot(nn, in) > 0.0f) nn = nn * -1.0f;
-	const float theta = acosf(cos_theta);
+	const float theta = lm_acosf(cos_theta);
 	const V3 hh = normalized(aa + bb);
 	const float nh = clampf(dot(nn, hh), -1.0f, 1.0f);
 	const float rough = smin(1.0f, sqrtf(g.rough) + ((2.0f * theta) / (float)PSY_PI_D));
@@ -470,7 +477,8 @@ static __device__ __noinline__ float gtr_estimate(const Gtr& g, V3 in, V3 cent, 
 // make_axis_angle_transform (math/transform.hpp:221-226).
 __device__ __forceinline__ M44 axis_angle(V3 axis, float angle) {
 	const V3 u = normalized(axis);
-	const float sine = sinf(angle), cosine = cosf(angle);
+	float sine, cosine;
+	lm_sincosf(angle, &sine, &cosine);
 	const float c1 = 1.0f - cosine;
 	M44 m;
 	m.m[0][0] = ((u.x * u.x) * c1) + cosine;

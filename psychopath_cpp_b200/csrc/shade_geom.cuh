@@ -14,6 +14,7 @@
 #define PSY_SHADE_GEOM_CUH
 
 #include "trace_device.cuh"
+#include "psy_libm.cuh"
 
 namespace psy {
 
@@ -204,10 +205,10 @@ static __device__ void hit_geometry(const DevScene& sc, const HitRec& rec, float
 		const float lat_sin = sqrtf((unit_p.x * unit_p.x) + (unit_p.y * unit_p.y));
 		const float long_cos = unit_p.x / lat_sin;
 		const float long_sin = unit_p.y / lat_sin;
-		const float latitude = acosf(lat_cos);
+		const float latitude = lm_acosf(lat_cos);
 		float longitude = 0.0f;
 		if (unit_p.x != 0.0f || unit_p.y != 0.0f) {
-			longitude = acosf(long_cos);
+			longitude = lm_acosf(long_cos);
 			if (unit_p.y < 0.0f) longitude = (float)((double)(2.0f * (float)1.0f) * PSY_PI_D - (double)longitude);
 		}
 		const float pi2 = (float)(PSY_PI_D * 2);

@@ -75,5 +75,5 @@ def test_reference_integrator_on_b200_trace(bridged_available, case):
     b = rx[..., 1].astype(np.float64)
     m = b > 1e-6 * b.max()
     err = float(np.sqrt(np.mean(((a[m] - b[m]) / b[m]) ** 2)))
-    assert m.sum() > 500
+    assert m.sum() > 0.1 * m.size  # lit pixels (most of the instanced frame is sky)
     assert err <= 1e-3, err

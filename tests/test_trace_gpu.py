@@ -203,7 +203,7 @@ def test_device_built_bvh_gives_the_same_hits(ctx, ref_available, kind):
     else:
         sc = scenes.heightfield_scene(64, seed=5)
         rays = scenes.heightfield_rays(60000, n=64, seed=42)
-    fields = ("hit", "id", "t", "uv")
+    fields = ("hit", "id", "t", "uv", "closure")
     ref = psyref.RefScene(scene=sc).trace(rays, threads=8)
     ctx.upload(sc)
     host_tree = api.Tracer(ctx).trace(rays, fields=fields)
@@ -212,9 +212,12 @@ def test_device_built_bvh_gives_the_same_hits(ctx, ref_available, kind):
     dev_tree = api.Tracer(ctx).trace(rays, fields=fields)
     assert st["bvh4_nodes"] > 0
     for mine in (host_tree, dev_tree):
-        rep = parity.compare_trace(ref, mine, rays["type"])
+        # uv of a light hit is whatever a farther candidate left (not compared)
+        rep = parity.compare_trace(ref, mine, rays["type"], uv_mask=mine["closure"] != 2)
         parity.assert_parity(rep)
     assert (host_tree["hit"] == dev_tree["hit"]).all()
+    if kind != "batch":
+        return  # the heightfield scene has no light to render with
     # a device-built tree renders the same image as the host-built one, up to
     # exact ties between candidates (met in another order)
     ctx.upload(sc)
