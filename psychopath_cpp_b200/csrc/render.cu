@@ -556,15 +556,13 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 		++c_warp;
 		c_lanes += __popc(run == 1 ? nmask : run == 2 ? lmask : pmask);
 		bool live = true;
-		if (run == 3) {
-			// bisections: every lane takes part in the warp-cooperative step,
-			// the lanes without one only in its votes
-			int left = PSY_PATCH_UNITS;
-			live = patch_step_warp<F>(w.scene(rid), st, kind == 3, left);
-			if (kind == 3) c_iters += PSY_PATCH_UNITS - left;
-		} else if (kind == run) {
+		if (kind == run) {
 			const DevScene& sc = w.scene(rid);
-			if (run == 1) {
+			if (run == 3) {
+				int left = PSY_PATCH_UNITS;
+				live = patch_step<F>(sc, st, left);
+				c_iters += PSY_PATCH_UNITS - left;
+			} else if (run == 1) {
 				int left = PSY_WALK_NODES;
 				const int r = walk_nodes<F>(sc, st, left);
 				c_nodes += PSY_WALK_NODES - left;

@@ -17,8 +17,6 @@
 #ifndef PSY_TRACE_DEVICE_CUH
 #define PSY_TRACE_DEVICE_CUH
 
-#include <type_traits>
-
 #include "psy_math.h"
 #include "psy_scene.h"
 
@@ -496,20 +494,13 @@ struct PatchCursor {
 	float u0, u1, v0, v1;
 	float t_nalpha, max_dim, h0, h1;
 	bool found;
-	// warp-cooperative walk (patch_units_warp): the lanes that walk this
-	// patch's split tree together, the first halves any of them left
-	// pending, whether this lane's ray hits the current node, and whether
-	// the lane has not joined a group yet
-	Bits128 gpend;
-	unsigned gmask;
-	bool act, fresh;
-	unsigned steps;  // group steps taken (bounded: PSY_PATCH_MAX_STEPS)
+	unsigned steps;  // loop iterations taken (bounded: PSY_PATCH_MAX_STEPS)
 };
 
-// A bisection ends with an error after this many group steps.  The walk is
-// finite (a leaf is forced at 63 second halves or depth 127), but a ray the
-// reference would bisect for hours must not hold a wave: far above any
-// bisection of a real scene.
+// A bisection ends with an error (ERRF_BISECT) after this many loop
+// iterations.  The walk is finite (a leaf is forced at 63 second halves or
+// depth 127), but a ray the reference would bisect for hours must not hold
+// a wave: far above any bisection of a real scene.
 #define PSY_PATCH_MAX_STEPS (1u << 24)
 
 // Sub-patches stored on the current path (with their uv ranges).
@@ -551,7 +542,7 @@ __device__ __forceinline__ bool patch_begin(PatchCursor<NV, TSC>& pc, const floa
 	pc.v0 = 0.0f;
 	pc.v1 = 1.0f;
 	pc.found = false;
-	pc.fresh = true;
+	pc.steps = 0;
 	return true;
 }
 
@@ -559,11 +550,14 @@ __device__ __forceinline__ bool patch_begin(PatchCursor<NV, TSC>& pc, const floa
 // split, with the resume that follows it).  Returns true when the
 // bisection has ended; pc.found then says whether a leaf was taken (the
 // closest one in *hit, with *max_t lowered to it; for occlusion rays the
-// first one).  Otherwise `pc` is the node to carry on from.
+// first one).  Otherwise `pc` is the node to carry on from.  A bisection
+// that exceeds PSY_PATCH_MAX_STEPS iterations ends without a hit and sets
+// ERRF_BISECT in *err.
 template <int NV, int TSC>
 __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<NV, TSC>& ps, const float* verts,
                                           const LocalRay& r, const RayWidth& rw, float* max_t, bool occl,
-                                          float dice_rate, float min_upoly, PatchHit* hit, int& units) {
+                                          float dice_rate, float min_upoly, PatchHit* hit, int& units,
+                                          unsigned* err) {
 	constexpr int CP = PSY_PATCH_CP_STEP;
 	constexpr int NCP = PSY_PATCH_CP_COUNT;
 	Patch<NV>(&cur)[TSC] = pc.cur;
@@ -578,6 +572,11 @@ __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<N
 	while (true) {
 		if (units == 0) return false;
 		--units;
+		if (++pc.steps > PSY_PATCH_MAX_STEPS) {
+			found = false;
+			*err |= ERRF_BISECT;
+			return true;
+		}
 		// `cur` is a node whose box the ray hits; max_dim, h0, h1 are its test
 		// A NaN width (from NaN ray differentials: a grazing hit makes the
 		// next ray's origin differentials 0/0 in transfer_ray_origin_
@@ -684,245 +683,17 @@ __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<N
 	}
 }
 
-// Sets `cur` (and its uv range) to the node at depth `depth` on `path`,
-// replayed from the deepest stored ancestor (or the root) with the splits
-// recorded in `dirs`: the same float operations as the walk down, so the
-// same control points.
-template <int NV, int TSC>
-__device__ __forceinline__ void patch_replay(Patch<NV> (&cur)[TSC], float& u0, float& u1, float& v0, float& v1,
-                                             const PatchStore<NV, TSC>& ps, const float* verts, const Bits128& path,
-                                             const Bits128& dirs, int depth) {
-	constexpr int CP = PSY_PATCH_CP_STEP;
-	constexpr int NCP = PSY_PATCH_CP_COUNT;
-	const int j = depth - 1;
-	int c = j / CP;
-	if (c > NCP) c = NCP;
-	if (c == 0) {
-#pragma unroll
-		for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur[k]);
-		u0 = 0.0f; u1 = 1.0f; v0 = 0.0f; v1 = 1.0f;
-	} else {
-#pragma unroll
-		for (int k = 0; k < TSC; ++k) cur[k] = ps.cps[c - 1][k];
-		u0 = ps.cpuv[c - 1][0]; u1 = ps.cpuv[c - 1][1]; v0 = ps.cpuv[c - 1][2]; v1 = ps.cpuv[c - 1][3];
-	}
-	for (int l = c * CP; l <= j; ++l) {
-		const bool second_half = path.get(l);
-		if (dirs.get(l)) {
-#pragma unroll
-			for (int k = 0; k < TSC; ++k) patch_half_u(cur[k], second_half);
-			const float um = (u0 + u1) * 0.5f;
-			if (second_half) u0 = um; else u1 = um;
-		} else {
-#pragma unroll
-			for (int k = 0; k < TSC; ++k) patch_half_v(cur[k], second_half);
-			const float vm = (v0 + v1) * 0.5f;
-			if (second_half) v0 = vm; else v1 = vm;
-		}
-	}
-}
-
-// Stores the node at `depth` when it is a checkpoint depth.
-template <int NV, int TSC>
-__device__ __forceinline__ void patch_checkpoint(PatchStore<NV, TSC>& ps, const Patch<NV> (&cur)[TSC], float u0,
-                                                 float u1, float v0, float v1, int depth) {
-	constexpr int CP = PSY_PATCH_CP_STEP;
-	constexpr int NCP = PSY_PATCH_CP_COUNT;
-	if (depth % CP == 0 && depth / CP <= NCP) {
-		const int c = depth / CP - 1;
-#pragma unroll
-		for (int k = 0; k < TSC; ++k) ps.cps[c][k] = cur[k];
-		ps.cpuv[c][0] = u0; ps.cpuv[c][1] = u1; ps.cpuv[c][2] = v0; ps.cpuv[c][3] = v1;
-	}
-}
-
-// Warp-cooperative bisection (the wave traversal kernels).  Every lane of
-// the warp calls it together (it votes with full-warp ballots); `in` says
-// whether the lane has a bisection of this patch kind in progress.  Lanes
-// that start the same patch at the same call form a group (match on the
-// patch's vertex pointer) and walk the patch's split tree together: the
-// group visits the union of the nodes its lanes would visit, in the same
-// depth-first order (second half first), and every node's split is made
-// once for the group, while each lane keeps its own ray, box tests, max t,
-// pending first halves and leaf decisions.  Restricted to the nodes a lane's
-// ray hits, the group's order is that lane's own walk (patch_run), so each
-// lane takes exactly the leaves it would take alone: the group only shares
-// control flow, so the lanes run converged instead of one by one.
-//
-// The group state (the node, its path, split directions and uv range, the
-// stored ancestors, the first halves any lane left pending) is computed
-// identically by every lane of the group; a lane whose ray hits neither half
-// of a split, or that is waiting for a first half, is inactive until the
-// group resumes at a node of its own.  A lane leaves its group when its own
-// walk has ended (no node of its own left); the others then drop it from
-// their mask in the same call, before it can join another group.
-//
-// Runs up to `units` group steps (a leaf test or split and the resumes that
-// follow).  Returns true for a lane whose bisection has ended (pc.found:
-// a leaf was taken, the closest in *hit with *max_t lowered to it).
-template <int NV, int TSC>
-__device__ __forceinline__ bool patch_units_warp(PatchCursor<NV, TSC>& pc, PatchStore<NV, TSC>& ps,
-                                                 const float* verts, const LocalRay& r, const RayWidth& rw,
-                                                 float* max_t, bool occl, float dice_rate, float min_upoly,
-                                                 PatchHit* hit, bool in, int& units, unsigned* err) {
-	constexpr unsigned FULL = 0xffffffffu;
-	const unsigned lane = threadIdx.x & 31u;
-	const bool start = in && pc.fresh;
-	const unsigned long long key =
-	    start ? (reinterpret_cast<unsigned long long>(verts) | (1ull << 63)) : (unsigned long long)lane;
-	const unsigned same = __match_any_sync(FULL, key);
-	if (start) {
-		pc.gmask = same;
-		pc.fresh = false;
-		pc.gpend = Bits128{0, 0};
-		pc.act = true;
-		pc.steps = 0;
-	}
-	bool done = false;
-	for (int u = 0; u < units; ++u) {
-		if (!__any_sync(FULL, in)) {
-			units -= u;
-			return done;
-		}
-		// leaf test of the lanes whose ray hits the node
-		bool fin = false;
-		if (in && ++pc.steps > PSY_PATCH_MAX_STEPS) {
-			// give up on this ray's bisection: the caller reports ERRF_BISECT
-			fin = true;
-			pc.act = false;
-			pc.pend = Bits128{0, 0};
-			pc.found = false;
-			*err |= ERRF_BISECT;
-		}
-		if (in && pc.act) {
-			const float wm = ray_min_width(rw, pc.h0, pc.h1) * dice_rate;
-			const float width = (wm != wm) ? min_upoly : smax(wm, min_upoly);
-			if (pc.max_dim <= width || pc.path.popc() == PSY_SPLIT_STACK - 1 || pc.depth == 127) {
-				const float tt = (pc.h0 + pc.h1) * 0.5f;
-				if (tt > 0.0f && tt < *max_t) {
-					pc.found = true;
-					if (occl) {
-						// an occlusion ray ends at its first leaf: nothing of
-						// its own is left for the group to resume
-						fin = true;
-						pc.pend = Bits128{0, 0};
-					} else {
-						*max_t = tt;
-						hit->t = tt;
-						hit->u = (pc.u0 + pc.u1) * 0.5f;
-						hit->v = (pc.v0 + pc.v1) * 0.5f;
-						hit->max_dim = pc.max_dim;
-					}
-				}
-				pc.act = false;
-			}
-		}
-		// the group splits the node when any of its lanes needs it split
-		const unsigned b_split = __ballot_sync(FULL, in && pc.act);
-		const bool gsplit = in && (b_split & pc.gmask) != 0u;
-		bool s_hit = false, f_hit = false, along_u = false;
-		Patch<NV> first[TSC];
-		float smd = 0.0f, sh0 = 0.0f, sh1 = 0.0f, fmd = 0.0f, fh0 = 0.0f, fh1 = 0.0f;
-		if (gsplit) {
-			along_u = patch_ulen(pc.cur[0]) > patch_vlen(pc.cur[0]);
-#pragma unroll
-			for (int k = 0; k < TSC; ++k) patch_split(pc.cur[k], first[k], along_u);
-			const bool sh = patch_node_test<NV, TSC>(pc.cur, pc.t_nalpha, r, *max_t, &smd, &sh0, &sh1);
-			const bool fh = patch_node_test<NV, TSC>(first, pc.t_nalpha, r, *max_t, &fmd, &fh0, &fh1);
-			s_hit = pc.act && sh;
-			f_hit = pc.act && fh;
-		}
-		const unsigned b_s = __ballot_sync(FULL, s_hit);
-		const unsigned b_f = __ballot_sync(FULL, f_hit);
-		bool resume = in && !gsplit;
-		if (gsplit) {
-			const bool any_s = (b_s & pc.gmask) != 0u, any_f = (b_f & pc.gmask) != 0u;
-			pc.dirs.set(pc.depth, along_u);
-			const float mid = along_u ? (pc.u0 + pc.u1) * 0.5f : (pc.v0 + pc.v1) * 0.5f;
-			if (any_s) {
-				pc.path.set(pc.depth, true);
-				pc.gpend.set(pc.depth, any_f);
-				pc.pend.set(pc.depth, f_hit);
-				pc.act = s_hit;
-				if (along_u) pc.u0 = mid; else pc.v0 = mid;
-				pc.max_dim = smd;
-				pc.h0 = sh0;
-				pc.h1 = sh1;
-			} else if (any_f) {
-				pc.path.set(pc.depth, false);
-#pragma unroll
-				for (int k = 0; k < TSC; ++k) pc.cur[k] = first[k];
-				pc.act = f_hit;
-				if (along_u) pc.u1 = mid; else pc.v1 = mid;
-				pc.max_dim = fmd;
-				pc.h0 = fh0;
-				pc.h1 = fh1;
-			} else {
-				// no lane's ray hits either half: the node is done for every
-				// lane of the group
-				pc.act = false;
-				resume = true;
-			}
-			if (any_s || any_f) {
-				++pc.depth;
-				patch_checkpoint<NV, TSC>(ps, pc.cur, pc.u0, pc.u1, pc.v0, pc.v1, pc.depth);
-			}
-		}
-		// resume at the deepest first half any lane of the group left pending
-		while (__any_sync(FULL, resume)) {
-			if (resume) {
-				const int j = pc.gpend.highest_below(pc.depth);
-				if (j < 0) {
-					resume = false;  // the group's walk has ended
-				} else {
-					pc.gpend.set(j, false);
-					pc.path.set(j, false);
-					pc.depth = j + 1;
-					pc.path.truncate(pc.depth);
-					pc.dirs.truncate(pc.depth);
-					pc.gpend.truncate(pc.depth);
-					const bool mine = pc.pend.get(j);
-					pc.pend.set(j, false);
-					pc.pend.truncate(pc.depth);
-					patch_replay<NV, TSC>(pc.cur, pc.u0, pc.u1, pc.v0, pc.v1, ps, verts, pc.path, pc.dirs, pc.depth);
-					patch_checkpoint<NV, TSC>(ps, pc.cur, pc.u0, pc.u1, pc.v0, pc.v1, pc.depth);
-					float md, a0, a1;
-					const bool hb = patch_node_test<NV, TSC>(pc.cur, pc.t_nalpha, r, *max_t, &md, &a0, &a1);
-					pc.max_dim = md;
-					pc.act = mine && hb;
-					if (pc.act) {
-						pc.h0 = a0;
-						pc.h1 = a1;
-					}
-				}
-			}
-			const unsigned b_act = __ballot_sync(FULL, resume && pc.act);
-			if (resume && (b_act & pc.gmask) != 0u) resume = false;
-		}
-		// a lane whose own walk has ended leaves its group
-		const bool leaving = in && (fin || (!pc.act && pc.pend.lo == 0ull && pc.pend.hi == 0ull));
-		const unsigned b_leave = __ballot_sync(FULL, leaving);
-		if (in) pc.gmask &= ~b_leave;
-		if (leaving) {
-			in = false;
-			done = true;
-		}
-	}
-	units = 0;
-	return done;
-}
-
 // The whole bisection of one patch in one call, its state in the caller's
 // frame.  Returns true when a leaf was taken.
 template <int NV, int TSC>
 __device__ bool patch_whole(const float* verts, float time, const LocalRay& r, const RayWidth& rw,
                                             float* max_t, bool occl, float dice_rate, float min_upoly,
-                                            PatchHit* hit) {
+                                            PatchHit* hit, unsigned* err) {
 	PatchCursor<NV, TSC> pc;
 	PatchStore<NV, TSC> ps;
 	if (!patch_begin<NV, TSC>(pc, verts, time, r, *max_t)) return false;
 	int units = 0x7fffffff;
-	patch_run<NV, TSC>(pc, ps, verts, r, rw, max_t, occl, dice_rate, min_upoly, hit, units);
+	patch_run<NV, TSC>(pc, ps, verts, r, rw, max_t, occl, dice_rate, min_upoly, hit, units, err);
 	return pc.found;
 }
 
@@ -1314,15 +1085,19 @@ __device__ __forceinline__ bool object_test(const DevScene& sc, TraceState<F>& s
 		if ((F & FEAT_BILINEAR) && ob.kind == OBJ_BILINEAR) {
 			const RayWidth w = width();
 			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-				hit = patch_whole<4, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_whole<4, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph,
+				                             &s.err);
 			else
-				hit = patch_whole<4, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_whole<4, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph,
+				                             &s.err);
 		} else if ((F & FEAT_BICUBIC) && ob.kind == OBJ_BICUBIC) {
 			const RayWidth w = width();
 			if ((F & FEAT_PATCH_MOTION) && ob.n0 != 1)
-				hit = patch_whole<16, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_whole<16, 2>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph,
+				                             &s.err);
 			else
-				hit = patch_whole<16, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph);
+				hit = patch_whole<16, 1>(v, wr.time, lr, w, &max_t, wr.occl, sc.dice_rate, sc.min_upoly_size, &ph,
+				                             &s.err);
 		}
 	} else {
 		begin_patch(v);
@@ -1417,7 +1192,7 @@ __device__ __forceinline__ bool patch_step(const DevScene& sc, TraceState<F>& s,
 	// state only when the bisection stops short of its end
 	auto run = [&](auto& pw) {
 		auto pc = pw.c;
-		done = patch_run(pc, pw.st, s.pverts, s.pr, s.prw, &max_t, occl, dr, mu, &s.ph, units);
+		done = patch_run(pc, pw.st, s.pverts, s.pr, s.prw, &max_t, occl, dr, mu, &s.ph, units, &s.err);
 		if (!done) pw.c = pc;
 		found = pc.found;
 	};
@@ -1429,50 +1204,6 @@ __device__ __forceinline__ bool patch_step(const DevScene& sc, TraceState<F>& s,
 		if (s.pmode == PM_BICUBIC1) run(s.template work<16, 1>());
 		else if (TS == 2 && s.pmode == PM_BICUBIC2) run(s.template work<16, TS>());
 	}
-	s.max_t = max_t;
-	if (!done) return true;
-	s.pmode = PM_NONE;
-	if (found) return trace_record<F>(s, s.p_obj, s.p_kind, s.p_id, s.p_shader, s.p_gi, s.ph);
-	return true;
-}
-
-// The warp-cooperative form of patch_step for the wave kernels: every lane
-// of the warp calls it together; `in` says whether the lane has a bisection
-// in progress.  Returns false for a lane whose ray is finished (an occlusion
-// ray's hit); `units` is left at the group steps the lane did not use.
-template <unsigned F>
-__device__ __forceinline__ bool patch_step_warp(const DevScene& sc, TraceState<F>& s, bool in, int& units) {
-	constexpr int TS = PatchBuf<F>::TS;
-	bool done = false, found = false;
-	float max_t = in ? s.max_t : 0.0f;
-	const bool occl = in && s.wr.occl;
-	const float dr = sc.dice_rate, mu = sc.min_upoly_size;
-	int used = 0;
-	// one call per compiled patch kind, made by every lane; a lane takes part
-	// in the call of its own kind only
-	auto run = [&](auto& pw, bool in_m) {
-		typename std::remove_reference<decltype(pw.c)>::type pc;
-		if (in_m) pc = pw.c;
-		int left = units;
-		const bool d = patch_units_warp(pc, pw.st, s.pverts, s.pr, s.prw, &max_t, occl, dr, mu, &s.ph, in_m, left,
-		                                &s.err);
-		if (in_m) {
-			done = d;
-			found = pc.found;
-			if (!d) pw.c = pc;
-			used = units - left;
-		}
-	};
-	if constexpr ((F & FEAT_BILINEAR) != 0) {
-		run(s.template work<4, 1>(), in && s.pmode == PM_BILINEAR1);
-		if constexpr (TS == 2) run(s.template work<4, TS>(), in && s.pmode == PM_BILINEAR2);
-	}
-	if constexpr ((F & FEAT_BICUBIC) != 0) {
-		run(s.template work<16, 1>(), in && s.pmode == PM_BICUBIC1);
-		if constexpr (TS == 2) run(s.template work<16, TS>(), in && s.pmode == PM_BICUBIC2);
-	}
-	units -= used;
-	if (!in) return true;
 	s.max_t = max_t;
 	if (!done) return true;
 	s.pmode = PM_NONE;
