@@ -74,8 +74,8 @@ __device__ __forceinline__ LocalRay make_local_x(const WorldRayD& wr, const M44&
 
 // The width parameters update_ray computes beside the local ray `r` (made
 // from wr with transform t, or none).  Computed once per space a ray meets
-// a patch in, so it is not inlined (smaller traversal code).
-static __device__ __noinline__ RayWidth ray_width_of(const WorldRayD& wr, const LocalRay& r, const M44* t) {
+// a patch in.
+__device__ __forceinline__ RayWidth ray_width_of(const WorldRayD& wr, const LocalRay& r, const M44* t) {
 	if (!t) return ray_width_params(r.o, r.d, wr.odx, wr.ody, wr.ddx, wr.ddy);
 	return ray_width_params(r.o, r.d, dir_to(*t, wr.odx), dir_to(*t, wr.ody), dir_to(*t, wr.ddx), dir_to(*t, wr.ddy));
 }
@@ -102,11 +102,10 @@ __device__ __forceinline__ M44 seq_lerp_global(const float* xs, int count, float
 // with instance transforms `b` (global, count nb), written into `dst`.
 // Returns false if the result needs more than PSY_MAX_MOTION samples.  The
 // three cases of the reference (equal counts, more parent samples, more
-// instance samples) share one loop with one matrix product, and the function
-// is not inlined: its callers run it rarely (entering a transformed
-// instance), and one copy of the code keeps the traversal kernels' code
-// small enough for the instruction cache.
-static __device__ __noinline__ bool frame_merge(const Frame& a, const float* b, int nb, Frame* dst) {
+// instance samples) share one loop with one matrix product.  (Outlined, so
+// that its frames pass through memory, this and the other traversal helpers
+// cost 11% of the many-light render's traversal time.)
+__device__ __forceinline__ bool frame_merge(const Frame& a, const float* b, int nb, Frame* dst) {
 	const int na = a.count;
 	if (na > PSY_MAX_MOTION || nb > PSY_MAX_MOTION) return false;
 	const int n = na > nb ? na : nb;
@@ -931,10 +930,9 @@ __device__ __forceinline__ void leave_levels(TraceState<F>& s) {
 // Enters the assembly of instance `inst` (global index gi, element id
 // `id`, inherited shader): merges its transforms into the level's frame,
 // moves the ray into its space and pushes its root.  Returns false when the
-// node stack overflows.  Not inlined: a ray enters few instances, and one
-// copy keeps the traversal kernels' code small.
+// node stack overflows.
 template <unsigned F>
-__device__ __noinline__ bool enter_assembly(const DevScene& sc, TraceState<F>& s, const DevInstance& inst, int gi,
+__device__ __forceinline__ bool enter_assembly(const DevScene& sc, TraceState<F>& s, const DevInstance& inst, int gi,
                                                uint64_t id, int shader) {
 	constexpr bool XFORM = (F & FEAT_XFORM) != 0;
 	const WorldRayD& wr = s.wr;
