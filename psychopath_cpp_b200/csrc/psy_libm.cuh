@@ -171,32 +171,32 @@ PSY_LM_HD float lm_acos_pq(float z) {
 	return p / q;
 }
 
+// The three ranges (|x| < 0.5, x < -0.5, x > 0.5) are evaluated with the
+// same operations as fdlibm's branches, but every lane computes the
+// rational function once and the square root and head/tail split once, and
+// the result is selected: the lanes of a warp take different ranges, and
+// branches would run the divisions once per range.
 PSY_LM_HD float lm_acosf(float x) {
 	using namespace psylm;
 	const float pi = 3.1415925026e+00f, pio2_hi = 1.5707962513e+00f, pio2_lo = 7.5497894159e-08f;
 	const uint32_t hx = fbits(x), ix = hx & 0x7fffffffu;
-	if (ix == 0x3f800000u) return (hx >> 31) ? pi + 2.0f * pio2_lo : 0.0f;
-	if (ix > 0x3f800000u) return (x - x) / (x - x);
-	if (ix < 0x3f000000u) {  // |x| < 0.5
-		if (ix <= 0x32800000u) return pio2_hi + pio2_lo;
-		const float r = lm_acos_pq(x * x);
-		return pio2_hi - (x - (pio2_lo - x * r));
+	if (ix >= 0x3f800000u) {  // |x| >= 1
+		if (ix == 0x3f800000u) return (hx >> 31) ? pi + 2.0f * pio2_lo : 0.0f;
+		return (x - x) / (x - x);
 	}
-	if (hx >> 31) {  // x < -0.5
-		const float z = (1.0f + x) * 0.5f;
-		const float s = sqrtf(z);
-		const float r = lm_acos_pq(z);
-		const float w = r * s - pio2_lo;
-		return pi - 2.0f * (s + w);
-	}
-	// x > 0.5: sqrt(z) split into a head with 12 low mantissa bits cleared
-	const float z = (1.0f - x) * 0.5f;
+	const bool small = ix < 0x3f000000u, neg = (hx >> 31) != 0;
+	const float z = small ? x * x : (neg ? (1.0f + x) * 0.5f : (1.0f - x) * 0.5f);
+	const float r = lm_acos_pq(z);
 	const float s = sqrtf(z);
+	// x > 0.5: sqrt(z) split into a head with 12 low mantissa bits cleared
 	const float df = bitsf(fbits(s) & 0xfffff000u);
 	const float c = (z - df * df) / (s + df);
-	const float r = lm_acos_pq(z);
-	const float w = r * s + c;
-	return 2.0f * (df + w);
+	const float a_small = ix <= 0x32800000u ? pio2_hi + pio2_lo : pio2_hi - (x - (pio2_lo - x * r));
+	const float w_neg = r * s - pio2_lo;
+	const float a_neg = pi - 2.0f * (s + w_neg);
+	const float w_pos = r * s + c;
+	const float a_pos = 2.0f * (df + w_pos);
+	return small ? a_small : (neg ? a_neg : a_pos);
 }
 
 // glibc's float asin: asin(t) ~ t + t^3 P(t^2), P of degree 4.
@@ -204,32 +204,33 @@ PSY_LM_HD float lm_asin_p(float t) {
 	return t * (1.666675248e-1f + t * (7.495297643e-2f + t * (4.547037598e-2f + t * (2.417951451e-2f + t * 4.216630880e-2f))));
 }
 
+// As lm_acosf, the ranges (|x| < 0.5, 0.5 <= |x| <= 0.975, above) share
+// the polynomial and the square root, and the result is selected.
 PSY_LM_HD float lm_asinf(float x) {
 	using namespace psylm;
 	const float pio2_hi = 1.57079637050628662109375f, pio2_lo = -4.37113900018624283e-8f,
 	            pio4_hi = 0.785398185253143310546875f;
 	const uint32_t hx = fbits(x), ix = hx & 0x7fffffffu;
-	if (ix == 0x3f800000u) return x * pio2_hi + x * pio2_lo;
-	if (ix > 0x3f800000u) return (x - x) / (x - x);
-	if (ix < 0x3f000000u) {  // |x| < 0.5
-		if (ix < 0x32000000u) return x;
-		const float w = lm_asin_p(x * x);
-		return x + x * w;
+	if (ix >= 0x3f800000u) {  // |x| >= 1
+		if (ix == 0x3f800000u) return x * pio2_hi + x * pio2_lo;
+		return (x - x) / (x - x);
 	}
+	const bool small = ix < 0x3f000000u;
 	const float w = 1.0f - fabsf(x);
-	float t = w * 0.5f;
-	float p = lm_asin_p(t);
+	const float t = small ? x * x : w * 0.5f;
+	const float p = lm_asin_p(t);
+	const float a_small = ix < 0x32000000u ? x : x + x * p;
 	const float s = sqrtf(t);
-	if (ix >= 0x3f79999au) {  // |x| > 0.975
-		t = pio2_hi - (2.0f * (s + s * p) - pio2_lo);
-	} else {
-		const float hw = bitsf(fbits(s) & 0xfffff000u);
-		const float c = (t - hw * hw) / (s + hw);
-		p = 2.0f * s * p - (pio2_lo - 2.0f * c);
-		const float q = pio4_hi - 2.0f * hw;
-		t = pio4_hi - (p - q);
-	}
-	return (hx >> 31) ? -t : t;
+	// |x| > 0.975
+	const float a_top = pio2_hi - (2.0f * (s + s * p) - pio2_lo);
+	// otherwise: sqrt(t) split into a head with 12 low mantissa bits cleared
+	const float hw = bitsf(fbits(s) & 0xfffff000u);
+	const float c = (t - hw * hw) / (s + hw);
+	const float pm = 2.0f * s * p - (pio2_lo - 2.0f * c);
+	const float q = pio4_hi - 2.0f * hw;
+	const float a_mid = pio4_hi - (pm - q);
+	const float a = ix >= 0x3f79999au ? a_top : a_mid;
+	return small ? a_small : ((hx >> 31) ? -a : a);
 }
 
 // expf: 2^(i/32) for i = 0..31 as the nearest double, less i << 47 (the

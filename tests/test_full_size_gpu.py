@@ -4,11 +4,12 @@ scene itself, against the reference's own code (oracle/_ref).
 * The 4,194,304-ray stream against the 256x256 bilinear heightfield (the
   trace benchmark, whole): per-ray parity (ids bit-exact, t/uv within 4 ulp).
 * The plain scene at 320x240, 16 spp, 4 segments (the CPU-runnable render,
-  whole): per-pixel relative RMSE <= 1e-3.
+  whole): per-pixel relative RMSE <= 1e-5 and the reference's ray count.
 * The 720p benchmark scene at full density (2,000 bicubic patches, 500
   instanced motion-blurred sphere groups, 10,000 sphere lights, depth of
   field, camera motion, 6 segments) on a 64x36 frame at 1024 spp:
-  per-pixel relative RMSE <= 1e-3, the image bar at 1024 spp.
+  per-pixel relative RMSE <= 1e-3, the image bar at 1024 spp, and in fact
+  <= 1e-5 with the reference's exact ray count (and so at 8 and 64 spp).
 
 The reference renders run in spawned child processes with a time limit: on
 some sampler seeds a ray with NaN differentials makes the reference's patch
@@ -29,6 +30,9 @@ from tests import parity
 pytestmark = pytest.mark.gpu
 
 IMAGE_REL_RMSE = 1e-3
+# renders here reproduce the reference path for path (the device restates
+# the host C library's float math): what is left is film summation order
+STRICT_REL_RMSE = 1e-5
 HEADLINE_SEEDS = (3, 4, 7, 8)
 
 
@@ -103,8 +107,8 @@ def test_plain_render_full_size(ctx, ref_available):
     assert (rc == mc).all()
     err, npx = rel_rmse(mx, rx)
     assert npx > 50000
-    assert err <= IMAGE_REL_RMSE, err
-    assert abs(int(rrays) - mrays) <= 0.001 * rrays, (rrays, mrays)
+    assert err <= STRICT_REL_RMSE, err
+    assert int(rrays) == int(mrays), (rrays, mrays)
 
 
 def _headline_kw(res):
@@ -114,18 +118,17 @@ def _headline_kw(res):
 @pytest.mark.parametrize("spp", [8, 64])
 def test_headline_scene_low_spp(ctx, ref_available, spp):
     """The benchmark scene at full density, 64x36, at 8 and 64 spp (seed 3):
-    the same sample sequences in both renderers; the error comes only from
-    the paths whose discrete choices flip on last-ulp differences, so it
-    shrinks as samples per pixel grow."""
+    the same sample sequences in both renderers, path for path."""
     kw = _headline_kw((64, 36))
     out = ref_render_bounded("many_light_scene", kw, spp, 6, HEADLINE_SEEDS[0], 600)
     assert out is not None, "reference render did not finish"
-    rx, rc, _ = out
-    mx, mc, _ = _render_ours(ctx, _scene("many_light_scene", kw), spp, 6, HEADLINE_SEEDS[0])
+    rx, rc, rrays = out
+    mx, mc, mrays = _render_ours(ctx, _scene("many_light_scene", kw), spp, 6, HEADLINE_SEEDS[0])
     assert (rc == mc).all()
     err, npx = rel_rmse(mx, rx)
     assert npx > 1500
-    assert err <= 2e-2, err
+    assert err <= STRICT_REL_RMSE, err
+    assert int(rrays) == int(mrays), (rrays, mrays)
 
 
 def test_headline_scene_1024spp(ctx, ref_available):
@@ -145,4 +148,6 @@ def test_headline_scene_1024spp(ctx, ref_available):
     err, npx = rel_rmse(mx, rx)
     assert npx > 1500
     assert err <= IMAGE_REL_RMSE, (seed, err)
-    assert abs(int(rrays) - mrays) <= 0.001 * rrays, (rrays, mrays)
+    # and path for path: the stated bar with two orders of magnitude to spare
+    assert err <= STRICT_REL_RMSE, (seed, err)
+    assert int(rrays) == int(mrays), (rrays, mrays)

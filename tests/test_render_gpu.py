@@ -3,8 +3,13 @@ reference's PathTraceIntegrator and LightTree::sample on the same scenes,
 seeds and Halton sequences.
 
 Image bar: per-pixel relative RMSE against the reference render <= 1e-3
-(paths are reproduced sample for sample; what remains are rare paths whose
-last-ulp differences flip a discrete choice, and film summation order).
+(the stated bar).  The paths are reproduced sample for sample, the float
+math included (the device restates the host C library's sincosf, acosf,
+asinf and expf), so the renders here also meet a much tighter bar:
+relative RMSE <= 1e-5 (what is left is film summation order and the last
+bits of intermediate products) and exactly the reference's ray count.
+GTR closures evaluate powf with CUDA's, which is not restated: their ray
+counts may differ by a few rays in 1e5.
 """
 import numpy as np
 import pytest
@@ -15,6 +20,7 @@ from tests import parity
 pytestmark = pytest.mark.gpu
 
 IMAGE_REL_RMSE = 1e-3
+STRICT_REL_RMSE = 1e-5
 
 
 def rel_rmse(mine, ref):
@@ -66,19 +72,13 @@ def test_light_tree_sample_parity(ctx, ref_available, which):
     ref_out, ref_ids = psyref.RefScene(scene=sc).light_sample(q)
     ctx.upload(sc)
     out, ids = api.LightTree(ctx).sample(q)
-    same = ref_ids == ids
-    # the light choice depends on sphere_lambert (asin/acos); allow rare flips
-    assert same.mean() > 0.999, same.mean()
-    for name, sl in (("to_light", slice(0, 3)), ("spec", slice(3, 7)), ("light_pdf", slice(9, 10))):
-        d = parity.ulp_diff(ref_out[same, sl], out[same, sl])
-        assert np.percentile(d, 99) <= 8, (name, np.percentile(d, 99), int(d.max()))
-    # selection_pdf multiplies one probability per tree level, each from
-    # sphere_lambert, whose g - h cancellation magnifies last-ulp differences
-    # of asinf/acosf between the host libm and the device
-    a = ref_out[same, 8].astype(np.float64)
-    b = out[same, 8].astype(np.float64)
-    rel = np.abs(a - b) / np.maximum(np.abs(a), 1e-30)
-    assert np.percentile(rel, 99.9) <= 1e-3, np.percentile(rel, 99.9)
+    # every light choice and every output bit equal: the tree walk's
+    # sphere_lambert takes asinf/acosf from the restated host library
+    assert (ref_ids == ids).all(), (ref_ids != ids).sum()
+    for name, sl in (("to_light", slice(0, 3)), ("spec", slice(3, 7)), ("selection_pdf", slice(8, 9)),
+                     ("light_pdf", slice(9, 10))):
+        d = parity.ulp_diff(ref_out[:, sl], out[:, sl])
+        assert d.max() == 0, (name, int((d > 0).sum()), int(d.max()))
 
 
 def test_plain_render_matches_reference(ctx, ref_available):
@@ -87,26 +87,26 @@ def test_plain_render_matches_reference(ctx, ref_available):
     assert (rc == mc).all()
     err, npx = rel_rmse(mx, rx)
     assert npx > 1000
-    assert err <= IMAGE_REL_RMSE, err
-    assert abs(int(rrays) - int(mrays)) <= 0.001 * rrays, (rrays, mrays)
+    assert err <= STRICT_REL_RMSE, err
+    assert int(rrays) == int(mrays), (rrays, mrays)
 
 
 def test_render_1024spp_relative_rmse(ctx, ref_available):
     sc = scenes.plain_scene(2, res=(32, 24), spp=1024)
-    (rx, rc, _), (mx, mc, _) = _render_both(ctx, sc, 1024, 4)
+    (rx, rc, rrays), (mx, mc, mrays) = _render_both(ctx, sc, 1024, 4)
     assert (rc == mc).all()
     err, _ = rel_rmse(mx, rx)
-    assert err <= IMAGE_REL_RMSE, err
+    assert err <= STRICT_REL_RMSE, err
+    assert int(rrays) == int(mrays), (rrays, mrays)
 
 
 def test_many_light_instanced_render(ctx, ref_available):
     sc = scenes.many_light_scene(7, res=(48, 27), spp=8, n_patches=80, n_groups=40, n_lights=500)
-    (rx, rc, _), (mx, mc, _) = _render_both(ctx, sc, 8, 6)
+    (rx, rc, rrays), (mx, mc, mrays) = _render_both(ctx, sc, 8, 6)
     assert (rc == mc).all()
     err, npx = rel_rmse(mx, rx)
-    # transformed instances use a correctly rounded matrix inverse where the
-    # reference uses an approximate-reciprocal one: a few ulp per vertex
-    assert err <= 1e-2, err
+    assert err <= STRICT_REL_RMSE, err
+    assert int(rrays) == int(mrays), (rrays, mrays)
 
 
 def test_motion_patch_render(ctx, ref_available):
@@ -117,8 +117,8 @@ def test_motion_patch_render(ctx, ref_available):
     assert (rc == mc).all()
     err, npx = rel_rmse(mx, rx)
     assert npx > 3000
-    assert err <= IMAGE_REL_RMSE, err
-    assert abs(int(rrays) - int(mrays)) <= 0.001 * rrays, (rrays, mrays)
+    assert err <= STRICT_REL_RMSE, err
+    assert int(rrays) == int(mrays), (rrays, mrays)
 
 
 def test_render_rejects_bad_arguments(ctx):
@@ -139,8 +139,8 @@ def test_rect_light_render(ctx, ref_available):
     assert (rc == mc).all()
     err, npx = rel_rmse(mx, rx)
     assert npx > 3000
-    assert err <= IMAGE_REL_RMSE, err
-    assert abs(int(rrays) - int(mrays)) <= 0.001 * rrays, (rrays, mrays)
+    assert err <= STRICT_REL_RMSE, err
+    assert int(rrays) == int(mrays), (rrays, mrays)
 
 
 def test_rect_light_sample_parity(ctx, ref_available):
@@ -150,11 +150,13 @@ def test_rect_light_sample_parity(ctx, ref_available):
     ref_out, ref_ids = psyref.RefScene(scene=sc).light_sample(q)
     ctx.upload(sc)
     out, ids = api.LightTree(ctx).sample(q)
-    same = ref_ids == ids
-    assert same.mean() > 0.999, same.mean()
-    for name, sl in (("to_light", slice(0, 3)), ("spec", slice(3, 7)), ("light_pdf", slice(9, 10))):
-        d = parity.ulp_diff(ref_out[same, sl], out[same, sl])
-        assert np.percentile(d, 99) <= 8, (name, np.percentile(d, 99), int(d.max()))
+    assert (ref_ids == ids).all(), (ref_ids != ids).sum()
+    for name, sl in (("to_light", slice(0, 3)), ("spec", slice(3, 7)), ("selection_pdf", slice(8, 9)),
+                     ("light_pdf", slice(9, 10))):
+        d = parity.ulp_diff(ref_out[:, sl], out[:, sl])
+        # to_light of the spherical-triangle sample goes through CUDA's
+        # double acos/sin/cos (not restated); a component in 1e4 may differ
+        assert (d > 0).mean() <= (1e-3 if name == "to_light" else 0.0), (name, int((d > 0).sum()), int(d.max()))
 
 
 def test_gtr_render(ctx, ref_available):
@@ -166,5 +168,6 @@ def test_gtr_render(ctx, ref_available):
     assert (rc == mc).all()
     err, npx = rel_rmse(mx, rx)
     assert npx > 3000
-    assert err <= IMAGE_REL_RMSE, err
-    assert abs(int(rrays) - int(mrays)) <= 0.001 * rrays, (rrays, mrays)
+    assert err <= STRICT_REL_RMSE, err
+    # powf (CUDA's) in the GTR distribution: a few rays in 1e5 may differ
+    assert abs(int(rrays) - int(mrays)) <= 1e-4 * rrays, (rrays, mrays)
