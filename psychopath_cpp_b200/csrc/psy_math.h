@@ -451,17 +451,8 @@ struct RayWidth {
 };
 
 // Width parameters of a ray with origin o, direction d and the (already
-// transformed) differentials.  Not inlined on the device: it runs once per
-// space a ray meets a patch in, and each of its IEEE divisions and square
-// roots expands to a long instruction sequence; its arguments and result
-// travel in registers.  (Inlined at its three call sites it made up a third
-// of the object-test code of the instanced-patch traversal kernel.)
-#ifdef __CUDACC__
-static __host__ __device__ __noinline__
-#else
-inline
-#endif
-RayWidth ray_width_params(V3 o, V3 d, V3 odx, V3 ody, V3 ddx, V3 ddy) {
+// transformed) differentials.
+PSY_HD RayWidth ray_width_params(V3 o, V3 d, V3 odx, V3 ody, V3 ddx, V3 ddy) {
 	RayWidth w;
 	float tdx, lx, tdy, ly;
 	closest_ray_t2(o, d, o + odx, d + ddx, &tdx, &lx);

@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 	unsigned rays = 0, c_nodes = 0, c_leaves = 0, c_iters = 0, c_warp = 0, c_lanes = 0;
 	TraceState<F> st;
 	int my = -1;    // queue position of this lane's ray, -1 = idle
-	bool at_leaf = false;  // walk_nodes stopped at a leaf (st.leaf)
+	int leaf = 0;   // walk_nodes stopped at a leaf (st.leaf): its LEAF_* class, else 0
 	int rid = 0;
 	bool more = true;  // the queue may still hold rays (warp-uniform)
 	while (true) {
@@ -536,40 +536,53 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 						rid = tag >> 1;
 						trace_init<F>(w.scene(rid), st, wr);
 						my = k;
-						at_leaf = false;
+						leaf = 0;
 						++rays;
 					}
 				}
 			}
 		}
-		// 0 = idle, 1 = node visits, 2 = leaf visit, 3 = bisection
-		const int kind = my < 0 ? 0 : st.pmode != PM_NONE ? 3 : at_leaf ? 2 : 1;
-		const unsigned nmask = __ballot_sync(0xffffffffu, kind == 1);
-		const unsigned lmask = __ballot_sync(0xffffffffu, kind == 2);
-		const unsigned pmask = __ballot_sync(0xffffffffu, kind == 3);
-		if ((nmask | lmask | pmask) == 0u) {
+		// KIND_IDLE, KIND_NODES (node visits), a leaf visit of one of the
+		// LEAF_* classes, or KIND_PATCH (bisection)
+		const int kind = my < 0 ? KIND_IDLE : st.pmode != PM_NONE ? KIND_PATCH : leaf ? leaf : KIND_NODES;
+		unsigned m[KIND_PATCH + 1];
+#pragma unroll
+		for (int k = KIND_NODES; k <= KIND_PATCH; ++k) m[k] = __ballot_sync(0xffffffffu, kind == k);
+		if ((m[KIND_NODES] | m[LEAF_ENTER] | m[LEAF_SIMPLE] | m[LEAF_PATCH] | m[KIND_PATCH]) == 0u) {
 			if (!more) break;
 			continue;
 		}
-		const int cn = __popc(nmask), cl = __popc(lmask) * PSY_LEAF_WEIGHT, cp = __popc(pmask) * PSY_PATCH_WEIGHT;
-		const int run = (cp >= cl && cp >= cn) ? 3 : (cl >= cn) ? 2 : 1;
+		// the kind most lanes have next (later kinds win ties)
+		int run = KIND_NODES, best = __popc(m[KIND_NODES]);
+#pragma unroll
+		for (int k = LEAF_ENTER; k <= KIND_PATCH; ++k) {
+			const int c = __popc(m[k]) * (k == KIND_PATCH ? PSY_PATCH_WEIGHT : PSY_LEAF_WEIGHT);
+			if (c >= best && c > 0) {
+				best = c;
+				run = k;
+			}
+		}
 		++c_warp;
-		c_lanes += __popc(run == 1 ? nmask : run == 2 ? lmask : pmask);
+		unsigned runmask = m[KIND_NODES];
+#pragma unroll
+		for (int k = LEAF_ENTER; k <= KIND_PATCH; ++k)
+			if (run == k) runmask = m[k];
+		c_lanes += __popc(runmask);
 		bool live = true;
 		if (kind == run) {
 			const DevScene& sc = w.scene(rid);
-			if (run == 3) {
+			if (run == KIND_PATCH) {
 				int left = PSY_PATCH_UNITS;
 				live = patch_step<F>(sc, st, left);
 				c_iters += PSY_PATCH_UNITS - left;
-			} else if (run == 1) {
+			} else if (run == KIND_NODES) {
 				int left = PSY_WALK_NODES;
 				const int r = walk_nodes<F>(sc, st, left);
 				c_nodes += PSY_WALK_NODES - left;
 				live = r != WALK_DONE;
-				at_leaf = r == WALK_LEAF;
+				leaf = r == WALK_LEAF ? leaf_class<F>(sc, st) : 0;
 			} else {
-				at_leaf = false;
+				leaf = 0;
 				++c_leaves;
 				live = leaf_visit<F>(sc, st);
 			}

@@ -1176,6 +1176,25 @@ __device__ __forceinline__ bool leaf_visit(const DevScene& sc, TraceState<F>& s)
 	return object_test<F, true>(sc, s, inst, gi, id, shader);
 }
 
+// Work kinds of the wave kernels' lanes: idle, node visits, a leaf visit of
+// one of three classes, a bisection in progress.  Leaf visits are told
+// apart by class so that the lanes of a warp step run one branch of
+// leaf_visit together: assembly entries (transform merge, ray transform),
+// simple objects (spheres, sphere and rectangle lights), patches (root box,
+// ray widths, bisection set-up).
+enum : int { KIND_IDLE = 0, KIND_NODES = 1, LEAF_ENTER = 2, LEAF_SIMPLE = 3, LEAF_PATCH = 4, KIND_PATCH = 5 };
+
+// The class of the leaf walk_nodes stopped at (s.leaf).
+template <unsigned F>
+__device__ __forceinline__ int leaf_class(const DevScene& sc, const TraceState<F>& s) {
+	constexpr bool NESTED = (F & FEAT_NESTED) != 0;
+	const int gi = s.lv[s.L].inst_base + leaf_instance(s.leaf);
+	const int2 kd = __ldg(reinterpret_cast<const int2*>(sc.instances + gi));  // kind, data
+	if (NESTED && kd.x == INST_ASSEMBLY) return LEAF_ENTER;
+	const int ok = __ldg(&sc.objects[kd.y].kind);
+	return (ok == OBJ_BICUBIC || ok == OBJ_BILINEAR) ? LEAF_PATCH : LEAF_SIMPLE;
+}
+
 // Carries the bisection in progress on for up to `units` iterations of its
 // loop (`units` is left at the iterations not used).  Returns false when
 // the ray is finished (an occlusion ray's hit).
