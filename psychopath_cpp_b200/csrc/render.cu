@@ -472,13 +472,24 @@ __global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, Wave
 //
 // Persistent warps with per-lane ray replacement: a lane whose ray is
 // finished takes the next ray of the queue between traversal steps instead
-// of idling until the slowest ray of its warp is done.  Two resident blocks
-// of 256 threads (128 registers a thread) hide more latency than the
-// register-unbounded variant's two blocks of 128 (measured: +13% on the
-// many-light scene, no change on flat scenes).
+// of idling until the slowest ray of its warp is done.  128 registers a
+// thread (16 resident warps an SM) hide more latency than the
+// register-unbounded variant's 8 warps (measured: +13% on the many-light
+// scene, no change on flat scenes).
+//
+// One block of PSY_TRACE_BLOCK threads per SM, whose warps run the same
+// kind of work while they can: the kernel is bound by instruction fetch
+// (the lanes of 16 warps spread over more code than an SM's instruction
+// cache holds), so a warp that has lanes for the kind the block is running
+// runs that kind, and only a warp without any takes its own most common
+// kind, which the block then follows.  The preference is a shared word
+// read and written without synchronisation (a stale value only costs
+// time).  Measured on the many-light render: 9% off the traversal time
+// against blocks of 128 threads that each vote alone.
 #ifndef PSY_REFILL_MIN
 #define PSY_REFILL_MIN 8  // idle lanes that trigger a refill while rays remain
 #endif
+#define PSY_TRACE_BLOCK 512
 // Each lane's traversal is cut into kinds of work: node visits (up to
 // PSY_WALK_NODES at a time, stopping at a leaf), leaf visits of three
 // classes (entering an assembly instance, testing a simple object, starting
@@ -504,7 +515,7 @@ __global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, Wave
 #endif
 
 template <class W, unsigned F, bool OCCL>
-__global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, const float4* __restrict__ rb,
+__global__ void __launch_bounds__(PSY_TRACE_BLOCK, 1) trace_wave_kernel(W w, WaveBufs wb, const float4* __restrict__ rb,
                                                          const int* n_dev, int n_host, int* work,
                                                          unsigned long long* counts, unsigned* status) {
 	const int n = n_dev ? *n_dev : n_host;
@@ -518,6 +529,9 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 	int leaf = 0;   // walk_nodes stopped at a leaf (st.leaf): its LEAF_* class, else 0
 	int rid = 0;
 	bool more = true;  // the queue may still hold rays (warp-uniform)
+	__shared__ int s_kind;  // the kind of work the block's warps run
+	if (threadIdx.x == 0) s_kind = KIND_NODES;
+	__syncthreads();
 	while (true) {
 		const unsigned idle = __ballot_sync(0xffffffffu, my < 0);
 		if (more && (__popc(idle) >= PSY_REFILL_MIN || idle == 0xffffffffu)) {
@@ -555,15 +569,25 @@ __global__ void __launch_bounds__(256, 2) trace_wave_kernel(W w, WaveBufs wb, co
 			if (!more) break;
 			continue;
 		}
-		// the kind most lanes have next (later kinds win ties)
-		int run = KIND_NODES, best = __popc(m[KIND_NODES]);
+		// the block's kind if this warp has lanes for it, else the kind most
+		// of its lanes have next (later kinds win ties), which the block takes
+		int run = *(volatile int*)&s_kind;
+		bool has = false;
 #pragma unroll
-		for (int k = LEAF_ENTER; k <= KIND_PATCH; ++k) {
-			const int c = __popc(m[k]) * (k == KIND_PATCH ? PSY_PATCH_WEIGHT : PSY_LEAF_WEIGHT);
-			if (c >= best && c > 0) {
-				best = c;
-				run = k;
+		for (int k = KIND_NODES; k <= KIND_PATCH; ++k)
+			if (run == k) has = m[k] != 0u;
+		if (!has) {
+			run = KIND_NODES;
+			int best = __popc(m[KIND_NODES]);
+#pragma unroll
+			for (int k = LEAF_ENTER; k <= KIND_PATCH; ++k) {
+				const int c = __popc(m[k]) * (k == KIND_PATCH ? PSY_PATCH_WEIGHT : PSY_LEAF_WEIGHT);
+				if (c >= best && c > 0) {
+					best = c;
+					run = k;
+				}
 			}
+			if (lane == 0) *(volatile int*)&s_kind = run;
 		}
 		++c_warp;
 		unsigned runmask = m[KIND_NODES];
@@ -966,8 +990,8 @@ static const WaveGrids& grids_for(int block) {
 	if (g[k].block != block) {
 		WaveGrids n;
 		n.block = block;
-		n.trace_c = persistent_grid(trace_wave_kernel<W, F, false>, block);
-		n.trace_o = persistent_grid(trace_wave_kernel<W, F, true>, block);
+		n.trace_c = persistent_grid(trace_wave_kernel<W, F, false>, PSY_TRACE_BLOCK);
+		n.trace_o = persistent_grid(trace_wave_kernel<W, F, true>, PSY_TRACE_BLOCK);
 		n.shade_c = persistent_grid(shade_hit_kernel<W, true, F>, block);
 		n.shade_b = persistent_grid(shade_hit_kernel<W, false, F>, block);
 		n.shadow = persistent_grid(shade_shadow_kernel<W>, block);
@@ -998,7 +1022,7 @@ static void launch_wave(const W& w, uint32_t path_length, const HaltonDev& hd, c
 	cudaMemsetAsync(c, 0, sizeof(int) * render_counter_count(path_length), st);
 	camera_gen_kernel<W><<<(P + block - 1) / block, block, 0, st>>>(w, hd, wv, ps, wb);
 	tstart();
-	trace_wave_kernel<W, F, false><<<g.trace_c, block, 0, st>>>(w, wb, wb.ray[0], nullptr, P, c + 0, wq.rays, status);
+	trace_wave_kernel<W, F, false><<<g.trace_c, PSY_TRACE_BLOCK, 0, st>>>(w, wb, wb.ray[0], nullptr, P, c + 0, wq.rays, status);
 	tstop();
 	// camera hit -> shadow rays of the live paths into queue 0
 	int* q = wq.q0;
@@ -1009,14 +1033,14 @@ static void launch_wave(const W& w, uint32_t path_length, const HaltonDev& hd, c
 	c += 4;
 	for (uint32_t b = 0; b < path_length; ++b) {
 		tstart();
-		trace_wave_kernel<W, F, true><<<g.trace_o, block, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays + TC_COUNT,
+		trace_wave_kernel<W, F, true><<<g.trace_o, PSY_TRACE_BLOCK, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays + TC_COUNT,
 		                                                          status);
 		tstop();
 		shade_shadow_kernel<W><<<g.shadow, block, gsmem, st>>>(w, hd, ps, wb, q, n, c + 1);
 		*launches += 2;
 		if (b + 1 == path_length) break;  // the last shadow step ends every path
 		tstart();
-		trace_wave_kernel<W, F, false><<<g.trace_c, block, 0, st>>>(w, wb, wb.ray[0], n, 0, c + 2, wq.rays, status);
+		trace_wave_kernel<W, F, false><<<g.trace_c, PSY_TRACE_BLOCK, 0, st>>>(w, wb, wb.ray[0], n, 0, c + 2, wq.rays, status);
 		tstop();
 		int* q2 = (q == wq.q0) ? wq.q1 : wq.q0;
 		int* n2 = c + 4;
