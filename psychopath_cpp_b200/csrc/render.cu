@@ -477,19 +477,27 @@ __global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, Wave
 // register-unbounded variant's 8 warps (measured: +13% on the many-light
 // scene, no change on flat scenes).
 //
-// One block of PSY_TRACE_BLOCK threads per SM, whose warps run the same
-// kind of work while they can: the kernel is bound by instruction fetch
-// (the lanes of 16 warps spread over more code than an SM's instruction
-// cache holds), so a warp that has lanes for the kind the block is running
-// runs that kind, and only a warp without any takes its own most common
-// kind, which the block then follows.  The preference is a shared word
-// read and written without synchronisation (a stale value only costs
-// time).  Measured on the many-light render: 9% off the traversal time
-// against blocks of 128 threads that each vote alone.
-#ifndef PSY_REFILL_MIN
-#define PSY_REFILL_MIN 8  // idle lanes that trigger a refill while rays remain
-#endif
-#define PSY_TRACE_BLOCK 512
+// Scenes with instance levels (the large traversal kernels): one block of
+// 512 threads per SM, whose warps run the same kind of work while they
+// can.  The kernel is bound by instruction fetch (the lanes of 16 warps
+// spread over more code than an SM's instruction cache holds), so a warp
+// that has lanes for the kind the block is running runs that kind, and
+// only a warp without any takes its own most common kind, which the block
+// then follows.  The preference is a shared word read and written without
+// synchronisation (a stale value only costs time).  A warp also refills
+// its lanes from 4 idle lanes instead of 8.  Measured on the many-light
+// render: 11% off the traversal time against blocks of 128 threads that
+// each vote alone.  Flat scenes (a small kernel) keep the render's block
+// size and the per-warp vote, which are 3-4% faster there.
+template <unsigned F>
+struct TraceCfg {
+	static constexpr bool NESTED = (F & FEAT_NESTED) != 0;
+	static constexpr int BLOCK = NESTED ? 512 : 256;      // launch bound (flat: the render's block size)
+	static constexpr int MIN_BLOCKS = NESTED ? 1 : 2;
+	static constexpr bool FOLLOW = NESTED;                // warps follow the block's kind of work
+	static constexpr int REFILL_MIN = NESTED ? 4 : 8;     // idle lanes that trigger a refill while rays remain
+	static int launch_block(int render_block) { return NESTED ? BLOCK : render_block; }
+};
 // Each lane's traversal is cut into kinds of work: node visits (up to
 // PSY_WALK_NODES at a time, stopping at a leaf), leaf visits of three
 // classes (entering an assembly instance, testing a simple object, starting
@@ -515,7 +523,7 @@ __global__ void __launch_bounds__(256) camera_gen_kernel(W w, HaltonDev hd, Wave
 #endif
 
 template <class W, unsigned F, bool OCCL>
-__global__ void __launch_bounds__(PSY_TRACE_BLOCK, 1) trace_wave_kernel(W w, WaveBufs wb, const float4* __restrict__ rb,
+__global__ void __launch_bounds__(TraceCfg<F>::BLOCK, TraceCfg<F>::MIN_BLOCKS) trace_wave_kernel(W w, WaveBufs wb, const float4* __restrict__ rb,
                                                          const int* n_dev, int n_host, int* work,
                                                          unsigned long long* counts, unsigned* status) {
 	const int n = n_dev ? *n_dev : n_host;
@@ -534,7 +542,7 @@ __global__ void __launch_bounds__(PSY_TRACE_BLOCK, 1) trace_wave_kernel(W w, Wav
 	__syncthreads();
 	while (true) {
 		const unsigned idle = __ballot_sync(0xffffffffu, my < 0);
-		if (more && (__popc(idle) >= PSY_REFILL_MIN || idle == 0xffffffffu)) {
+		if (more && (__popc(idle) >= TraceCfg<F>::REFILL_MIN || idle == 0xffffffffu)) {
 			int base = 0;
 			if (lane == 0) base = atomicAdd(work, __popc(idle));
 			base = __shfl_sync(0xffffffffu, base, 0);
@@ -573,9 +581,11 @@ __global__ void __launch_bounds__(PSY_TRACE_BLOCK, 1) trace_wave_kernel(W w, Wav
 		// of its lanes have next (later kinds win ties), which the block takes
 		int run = *(volatile int*)&s_kind;
 		bool has = false;
+		if (TraceCfg<F>::FOLLOW) {
 #pragma unroll
-		for (int k = KIND_NODES; k <= KIND_PATCH; ++k)
-			if (run == k) has = m[k] != 0u;
+			for (int k = KIND_NODES; k <= KIND_PATCH; ++k)
+				if (run == k) has = m[k] != 0u;
+		}
 		if (!has) {
 			run = KIND_NODES;
 			int best = __popc(m[KIND_NODES]);
@@ -587,7 +597,7 @@ __global__ void __launch_bounds__(PSY_TRACE_BLOCK, 1) trace_wave_kernel(W w, Wav
 					run = k;
 				}
 			}
-			if (lane == 0) *(volatile int*)&s_kind = run;
+			if (TraceCfg<F>::FOLLOW && lane == 0) *(volatile int*)&s_kind = run;
 		}
 		++c_warp;
 		unsigned runmask = m[KIND_NODES];
@@ -979,6 +989,7 @@ static int persistent_grid(K kernel, int block) {
 
 struct WaveGrids {
 	int block = 0;
+	int trace_b = 0;  // traversal block size
 	int trace_c, trace_o, shade_c, shade_b, shadow;
 };
 
@@ -990,8 +1001,9 @@ static const WaveGrids& grids_for(int block) {
 	if (g[k].block != block) {
 		WaveGrids n;
 		n.block = block;
-		n.trace_c = persistent_grid(trace_wave_kernel<W, F, false>, PSY_TRACE_BLOCK);
-		n.trace_o = persistent_grid(trace_wave_kernel<W, F, true>, PSY_TRACE_BLOCK);
+		n.trace_b = TraceCfg<F>::launch_block(block);
+		n.trace_c = persistent_grid(trace_wave_kernel<W, F, false>, n.trace_b);
+		n.trace_o = persistent_grid(trace_wave_kernel<W, F, true>, n.trace_b);
 		n.shade_c = persistent_grid(shade_hit_kernel<W, true, F>, block);
 		n.shade_b = persistent_grid(shade_hit_kernel<W, false, F>, block);
 		n.shadow = persistent_grid(shade_shadow_kernel<W>, block);
@@ -1022,7 +1034,7 @@ static void launch_wave(const W& w, uint32_t path_length, const HaltonDev& hd, c
 	cudaMemsetAsync(c, 0, sizeof(int) * render_counter_count(path_length), st);
 	camera_gen_kernel<W><<<(P + block - 1) / block, block, 0, st>>>(w, hd, wv, ps, wb);
 	tstart();
-	trace_wave_kernel<W, F, false><<<g.trace_c, PSY_TRACE_BLOCK, 0, st>>>(w, wb, wb.ray[0], nullptr, P, c + 0, wq.rays, status);
+	trace_wave_kernel<W, F, false><<<g.trace_c, g.trace_b, 0, st>>>(w, wb, wb.ray[0], nullptr, P, c + 0, wq.rays, status);
 	tstop();
 	// camera hit -> shadow rays of the live paths into queue 0
 	int* q = wq.q0;
@@ -1033,14 +1045,14 @@ static void launch_wave(const W& w, uint32_t path_length, const HaltonDev& hd, c
 	c += 4;
 	for (uint32_t b = 0; b < path_length; ++b) {
 		tstart();
-		trace_wave_kernel<W, F, true><<<g.trace_o, PSY_TRACE_BLOCK, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays + TC_COUNT,
+		trace_wave_kernel<W, F, true><<<g.trace_o, g.trace_b, 0, st>>>(w, wb, wb.ray[1], n, 0, c + 0, wq.rays + TC_COUNT,
 		                                                          status);
 		tstop();
 		shade_shadow_kernel<W><<<g.shadow, block, gsmem, st>>>(w, hd, ps, wb, q, n, c + 1);
 		*launches += 2;
 		if (b + 1 == path_length) break;  // the last shadow step ends every path
 		tstart();
-		trace_wave_kernel<W, F, false><<<g.trace_c, PSY_TRACE_BLOCK, 0, st>>>(w, wb, wb.ray[0], n, 0, c + 2, wq.rays, status);
+		trace_wave_kernel<W, F, false><<<g.trace_c, g.trace_b, 0, st>>>(w, wb, wb.ray[0], n, 0, c + 2, wq.rays, status);
 		tstop();
 		int* q2 = (q == wq.q0) ? wq.q1 : wq.q0;
 		int* n2 = c + 4;
