@@ -650,9 +650,21 @@ __global__ void __launch_bounds__(TraceCfg<F>::BLOCK, TraceCfg<F>::MIN_BLOCKS) t
 // After a camera (CAMERA) or bounce ray: update_path
 // (path_trace_integrator.cpp:251-272 and 273-302), then the shadow step of
 // next_ray_for_path (path_trace_integrator.cpp:126-184).
+//
+// Registers are capped at PSY_SHADE_MAXNREG a thread.  The kernel waits on
+// memory (path state, light-tree nodes, light and shader records) through
+// long dependent chains, and with the compiler's choice of about 225
+// registers only 8 warps fit an SM; at 32 registers 64 fit, and the spills
+// stay in L1.  Measured (640x360x4 many-light frame / flat 20,000- and
+// 50,000-primitive renders): 95.2 -> 84.4 ms and 45.2 -> 23.1 and
+// 96.5 -> 47.5 ms for the whole render, with caps of 168, 128, 96, 64, 48
+// and 40 registers in between.
 // ---------------------------------------------------------------------
+#ifndef PSY_SHADE_MAXNREG
+#define PSY_SHADE_MAXNREG 32
+#endif
 template <class W, bool CAMERA, unsigned F>
-__global__ void __launch_bounds__(256) shade_hit_kernel(W w, HaltonDev hd, PathSoA ps, WaveBufs wb,
+__global__ void __maxnreg__(PSY_SHADE_MAXNREG) shade_hit_kernel(W w, HaltonDev hd, PathSoA ps, WaveBufs wb,
                                                         const int* __restrict__ q_in, const int* n_dev, int n_host,
                                                         int* q_out, int* n_out, int* work, unsigned* status) {
 	extern __shared__ float sgrad[];
