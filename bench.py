@@ -792,6 +792,61 @@ def run_adjoint_ours(args, rank, local, pg, world):
     }
 
 
+def run_batch_small(local) -> dict:
+    """Many small renders (previews): 48 renders of 64x64 to 256x192 at 4 to
+    16 spp, 100 to 5,000 primitives, psy_render_batch (autotuned, graph)
+    against one psy_render per render, each timed over 5 passes with CUDA
+    events.  This is the case batching is for: one render alone leaves most
+    of the GPU idle."""
+    import torch
+    from psychopath_cpp_b200 import api, scenes
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(5)
+    entries = []
+    for i in range(48):
+        res = [(64, 64), (128, 96), (160, 120), (256, 192)][i % 4]
+        spp = int(rng.choice([4, 8, 16]))
+        ctx = api.Context(local)
+        ctx.upload(scenes.batch_scene(100 + i, res, spp, int(rng.integers(100, 5000)), int(rng.integers(1, 20))))
+        entries.append({"scene": ctx, "width": res[0], "height": res[1], "spp": spp, "seed": i + 1, "path_length": 4})
+    paths = sum(e["width"] * e["height"] * e["spp"] for e in entries)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    integs = [api.PathTraceIntegrator(e["scene"], e["width"], e["height"], e["spp"], seed=e["seed"], path_length=4)
+              for e in entries]
+    films = [(torch.zeros(e["width"] * e["height"] * 3, device=dev),
+              torch.zeros(e["width"] * e["height"], dtype=torch.int32, device=dev)) for e in entries]
+
+    def plain():
+        for it, (x, c) in zip(integs, films):
+            it.integrate_device(x, c, sp, with_stats=False)
+
+    def timed(fn, n=5):
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(n):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        return s.elapsed_time(e) / n
+
+    for _ in range(2):
+        plain()
+    plain_ms = timed(plain)
+    owner = api.Context(local)
+    b = api.BatchRenderer(owner, entries, use_graph=True)
+    tune = b.autotune(spp_divisor=1)
+    rb = lambda: b.render(sp, with_stats=False)
+    for _ in range(2):
+        rb()
+    batch_ms = timed(rb)
+    return {"value": round(plain_ms / batch_ms, 3), "batched_paths_per_s": round(paths / (batch_ms * 1e-3), 1),
+            "plain_paths_per_s": round(paths / (plain_ms * 1e-3), 1), "paths": paths, "tuned": tune,
+            "workload": "48 small renders: 64x64..256x192, 4-16 spp, 100-5,000 primitives, 1-19 lights, 4 segments",
+            "steps": 5}
+
+
 def render_line_extras(args, rank, local, pg, world) -> dict:
     """The other two figures of the headline metric, measured after the
     render's timed region, each with its own CUDA events and clock record:
@@ -803,6 +858,7 @@ def render_line_extras(args, rank, local, pg, world) -> dict:
     out["batched_over_plain"] = {"value": b["batched_over_plain"], "batched_paths_per_s": b["value"],
                                  "plain_paths_per_s": b["plain_paths_per_s"], "workload": b["config"]["workload"],
                                  "steps": 1, "clocks": b["clocks"]}
+    out["batched_over_plain"]["small_renders"] = run_batch_small(local)
     small.steps, small.warmup = 10, 3
     a = run_adjoint_ours(small, rank, local, pg, world)
     out["adjoint_over_forward"] = {"value": a["value"], "forward_ms": a["forward_ms"], "adjoint_ms": a["adjoint_ms"],

@@ -484,7 +484,7 @@ typedef struct psy_batch_tuning {
 
 /* Autotuner: times the batch with every sample count divided by
  * spp_divisor (at least 1; scratch films, the batch's films are not
- * touched) for waves of 2^14..2^20 paths and blocks of 64, 128 and 256
+ * touched) for waves of 2^14..2^22 paths and blocks of 64, 128 and 256
  * threads, keeps the fastest in ctx for psy_render_batch calls whose
  * configuration fields are 0, and returns it.  Synchronous. */
 int psy_batch_autotune(psy_ctx* ctx, const psy_batch_desc* batch, uint32_t spp_divisor, psy_batch_tuning* out);

@@ -936,7 +936,7 @@ int psy_batch_autotune(psy_ctx* ctx, const psy_batch_desc* b, uint32_t spp_divis
 	psy_batch_tuning best{};
 	best.ms = -1.0f;
 	uint32_t trials = 0;
-	for (uint32_t lg = 14; lg <= 20 && rc == PSY_OK; ++lg) {
+	for (uint32_t lg = 14; lg <= 22 && rc == PSY_OK; ++lg) {
 		for (uint32_t bi = 0; bi < 3; ++bi) {
 			t.stream_paths = 1u << lg;
 			t.block_size = blocks[bi];

