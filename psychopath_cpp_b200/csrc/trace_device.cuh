@@ -454,16 +454,9 @@ __device__ __forceinline__ bool patch_node_test(const Patch<NV> (&q)[TSC], float
 	return h && !(*h1 != *h1);
 }
 
-// Sub-patches stored on the current path: one every PSY_PATCH_CP_STEP
-// levels, for depths PSY_PATCH_CP_STEP .. PSY_PATCH_CP_STEP*PSY_PATCH_CP_COUNT.
-// A resume replays at most PSY_PATCH_CP_STEP - 1 half splits from the
-// nearest stored one.  (Measured on the many-light render, 12 traversal
-// launches of a 640x360x4 frame: every 8 levels 74.3 ms, 4 71.6 ms, 3
-// 70.9 ms, 2 69.4 ms; flat scenes the same.)
-#ifndef PSY_PATCH_CP_STEP
-#define PSY_PATCH_CP_STEP 2
-#define PSY_PATCH_CP_COUNT 28
-#endif
+// Pending first halves a bisection can hold: at most one per second half
+// on the path, and the path has at most PSY_SPLIT_STACK - 1 of those.
+#define PSY_PATCH_PEND PSY_SPLIT_STACK
 
 // Per-ray bisection of one patch with TSC time samples (TSC = 1 or 2):
 // intersect_rays_with_patch for a single ray (object/patch_utils.hpp:18-200).
@@ -472,24 +465,23 @@ __device__ __forceinline__ bool patch_node_test(const Patch<NV> (&q)[TSC], float
 // a split pushes the first half, then the second, and the second half is
 // processed first.  Here both halves are tested against the ray when they
 // are made.  The second half is entered if its box is hit; the first half
-// is entered at once if only its box is hit, remembered as pending if both
-// are, and dropped if its box is missed (box_hit only gets stricter as the
-// ray's max t shrinks, so the reference would find it missed later as well).
-// A node is its path from the root (1 = second half) plus the split
-// directions; a pending first half is rebuilt when its turn comes by
-// replaying the recorded splits from the deepest stored ancestor on the path
-// (every PSY_PATCH_CP_STEP levels, else the root).  The replay performs the
-// same float operations as the first split, so every node's control points
-// and uv range are bit-identical to the reference's, the visiting order and
-// the leaf results are the same, and no per-ray stack of sub-patches is
-// needed.  The reference's stack index (its forced leaf at 63) is the number
-// of second halves on the path: the population count of the path bits.
+// is entered at once if only its box is hit, pushed on a stack of pending
+// first halves (control points and uv range) if both are, and dropped if
+// its box is missed (box_hit only gets stricter as the ray's max t
+// shrinks, so the reference would find it missed later as well).  When a
+// subtree ends, the deepest pending first half is popped and tested again
+// with the current max t.  The stack holds only the halves that are
+// pending, so it is written once per split that hits both halves; the path
+// bits (1 = second half) give the reference's stack index (its forced leaf
+// at 63: the population count of the path) and the depth to resume at.
+// Control points and uv ranges are those of the reference's walk, so the
+// visiting order and the leaf results are the same.
 //
 // The bisection can stop after any number of loop iterations and resume
 // later from its cursor (the node at the top of the loop, whose box the ray
-// hits, with its path bits and uv range) and its stored ancestors, so that
-// a lane can leave a long bisection to run with the other lanes of its
-// warp.  patch_run works on a cursor the caller holds as a local (kept in
+// hits, with its path bits and uv range) and its stack, so that a lane can
+// leave a long bisection to run with the other lanes of its warp.
+// patch_run works on a cursor the caller holds as a local (kept in
 // registers) and copies back only when it stops short of the end.
 template <int NV, int TSC>
 struct PatchCursor {
@@ -500,6 +492,7 @@ struct PatchCursor {
 	float t_nalpha, max_dim, h0, h1;
 	bool found;
 	unsigned steps;  // loop iterations taken (bounded: PSY_PATCH_MAX_STEPS)
+	int sp;          // pending first halves on the stack
 };
 
 // A bisection ends with an error (ERRF_BISECT) after this many loop
@@ -511,8 +504,8 @@ struct PatchCursor {
 // Sub-patches stored on the current path (with their uv ranges).
 template <int NV, int TSC>
 struct PatchStore {
-	Patch<NV> cps[PSY_PATCH_CP_COUNT][TSC];
-	float cpuv[PSY_PATCH_CP_COUNT][4];
+	Patch<NV> pend[PSY_PATCH_PEND][TSC];
+	float penduv[PSY_PATCH_PEND][4];
 };
 
 // A suspended bisection in a lane's traversal state.
@@ -548,6 +541,7 @@ __device__ __forceinline__ bool patch_begin(PatchCursor<NV, TSC>& pc, const floa
 	pc.v1 = 1.0f;
 	pc.found = false;
 	pc.steps = 0;
+	pc.sp = 0;
 	return true;
 }
 
@@ -563,8 +557,6 @@ __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<N
                                           const LocalRay& r, const RayWidth& rw, float* max_t, bool occl,
                                           float dice_rate, float min_upoly, PatchHit* hit, int& units,
                                           unsigned* err) {
-	constexpr int CP = PSY_PATCH_CP_STEP;
-	constexpr int NCP = PSY_PATCH_CP_COUNT;
 	Patch<NV>(&cur)[TSC] = pc.cur;
 	const float t_nalpha = pc.t_nalpha;
 	float &max_dim = pc.max_dim, &h0 = pc.h0, &h1 = pc.h1;
@@ -572,8 +564,6 @@ __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<N
 	int& depth = pc.depth;
 	float &u0 = pc.u0, &u1 = pc.u1, &v0 = pc.v0, &v1 = pc.v1;
 	bool& found = pc.found;
-	auto& cps = ps.cps;
-	auto& cpuv = ps.cpuv;
 	while (true) {
 		if (units == 0) return false;
 		--units;
@@ -616,6 +606,16 @@ __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<N
 			if (s_hit) {
 				path.set(depth, true);
 				pend.set(depth, f_hit);
+				if (f_hit) {
+					// the first half waits on the stack with its uv range
+					const int q = pc.sp++;
+#pragma unroll
+					for (int k = 0; k < TSC; ++k) ps.pend[q][k] = first[k];
+					ps.penduv[q][0] = u0;
+					ps.penduv[q][1] = along_u ? mid : u1;
+					ps.penduv[q][2] = v0;
+					ps.penduv[q][3] = along_u ? v1 : mid;
+				}
 				if (along_u) u0 = mid; else v0 = mid;
 				max_dim = smd;
 				h0 = sh0;
@@ -633,16 +633,11 @@ __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<N
 			}
 			if (entered) {
 				++depth;
-				if (depth % CP == 0 && depth / CP <= NCP) {
-					const int c = depth / CP - 1;
-#pragma unroll
-					for (int k = 0; k < TSC; ++k) cps[c][k] = cur[k];
-					cpuv[c][0] = u0; cpuv[c][1] = u1; cpuv[c][2] = v0; cpuv[c][3] = v1;
-				}
 				continue;
 			}
 		}
-		// resume at the deepest pending first half whose box is still hit
+		// resume at the deepest pending first half (the top of the stack)
+		// whose box is still hit
 		while (true) {
 			const int j = pend.highest_below(depth);
 			if (j < 0) return true;
@@ -652,37 +647,10 @@ __device__ __forceinline__ bool patch_run(PatchCursor<NV, TSC>& pc, PatchStore<N
 			path.truncate(depth);
 			dirs.truncate(depth);
 			pend.truncate(depth);
-			int c = j / CP;
-			if (c > NCP) c = NCP;
-			if (c == 0) {
+			const int q = --pc.sp;
 #pragma unroll
-				for (int k = 0; k < TSC; ++k) patch_load<NV>(verts + k * NV * 3, &cur[k]);
-				u0 = 0.0f; u1 = 1.0f; v0 = 0.0f; v1 = 1.0f;
-			} else {
-#pragma unroll
-				for (int k = 0; k < TSC; ++k) cur[k] = cps[c - 1][k];
-				u0 = cpuv[c - 1][0]; u1 = cpuv[c - 1][1]; v0 = cpuv[c - 1][2]; v1 = cpuv[c - 1][3];
-			}
-			for (int l = c * CP; l <= j; ++l) {
-				const bool second_half = path.get(l);  // 0 at level j: the first half
-				if (dirs.get(l)) {
-#pragma unroll
-					for (int k = 0; k < TSC; ++k) patch_half_u(cur[k], second_half);
-					const float um = (u0 + u1) * 0.5f;
-					if (second_half) u0 = um; else u1 = um;
-				} else {
-#pragma unroll
-					for (int k = 0; k < TSC; ++k) patch_half_v(cur[k], second_half);
-					const float vm = (v0 + v1) * 0.5f;
-					if (second_half) v0 = vm; else v1 = vm;
-				}
-			}
-			if (depth % CP == 0 && depth / CP <= NCP) {
-				const int s = depth / CP - 1;
-#pragma unroll
-				for (int k = 0; k < TSC; ++k) cps[s][k] = cur[k];
-				cpuv[s][0] = u0; cpuv[s][1] = u1; cpuv[s][2] = v0; cpuv[s][3] = v1;
-			}
+			for (int k = 0; k < TSC; ++k) cur[k] = ps.pend[q][k];
+			u0 = ps.penduv[q][0]; u1 = ps.penduv[q][1]; v0 = ps.penduv[q][2]; v1 = ps.penduv[q][3];
 			if (patch_node_test<NV, TSC>(cur, t_nalpha, r, *max_t, &max_dim, &h0, &h1)) break;
 		}
 	}
