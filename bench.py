@@ -41,7 +41,7 @@ BYTES_PER_OCCLUSION_RAY = 64
 # DRAM bytes per traced ray of the traversal kernel, from the ncu capture in
 # profiles/trace_wave_kernel_many_light_640x360x4.md (dram read + write of the
 # camera launch / its 921,600 rays)
-TRAFFIC_BYTES_PER_RAY = 22398.0
+TRAFFIC_BYTES_PER_RAY = 13396.0
 BYTES_PER_PATH_EXTRA = 20   # sampler seed 4 + pixel 4 + XYZ 12
 RENDER_RES = (1280, 720)
 RENDER_SPP = 64
