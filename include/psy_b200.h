@@ -153,10 +153,13 @@ int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* scene);
 #define PSY_UPLOAD_GPU_BVH 1u
 int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* scene, uint32_t flags);
 
-/* Summary of the uploaded scene (for tests and tooling). */
+/* Summary of the uploaded scene (for tests and tooling).  gpu_bvh4_nodes and
+ * gpu_light_nodes count the nodes of bvh4_nodes and light_nodes that the
+ * device built (PSY_UPLOAD_GPU_BVH), 0 when the host built them all. */
 typedef struct psy_scene_stats {
 	uint32_t assemblies, instances, objects, bvh4_nodes, light_nodes, lights;
 	uint64_t device_bytes;
+	uint32_t gpu_bvh4_nodes, gpu_light_nodes;
 } psy_scene_stats;
 int psy_scene_stats_get(const psy_ctx* ctx, psy_scene_stats* out);
 

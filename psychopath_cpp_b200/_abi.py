@@ -83,7 +83,7 @@ class SceneDesc(C.Structure):
 class SceneStats(C.Structure):
     _fields_ = [("assemblies", C.c_uint32), ("instances", C.c_uint32), ("objects", C.c_uint32),
                 ("bvh4_nodes", C.c_uint32), ("light_nodes", C.c_uint32), ("lights", C.c_uint32),
-                ("device_bytes", C.c_uint64)]
+                ("device_bytes", C.c_uint64), ("gpu_bvh4_nodes", C.c_uint32), ("gpu_light_nodes", C.c_uint32)]
 
 
 class RaySoA(C.Structure):

@@ -166,6 +166,14 @@ cudaError_t launch_trace(const DevScene& sc, const RaySoA& rays, const HitSoA& h
 cudaError_t build_bvh4_gpu(const float* h_boxes, int n, int node_base, DevNode* d_nodes, int* root_ref,
                            int* node_count, cudaStream_t st);
 
+// Device build of a light tree over n lights (host, 11 floats each, see
+// BuiltScene::gpu_light_elems) into d_nodes[0 .. 2n - 2], numbered from
+// node_base in their child references, time-sample extra index `extra`;
+// *root_energy receives the root's energy.  Synchronous on `st`
+// (light_gpu.cu).
+cudaError_t build_light_tree_gpu(const float* h_elems, int n, int node_base, int extra, DevLightNode* d_nodes,
+                                 float* root_energy, cudaStream_t st);
+
 }  // namespace psy
 
 #endif

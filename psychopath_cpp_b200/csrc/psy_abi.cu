@@ -597,13 +597,38 @@ int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags
 	} else {
 		UP(nodes, b->nodes);
 	}
+	ctx->gpu_light_nodes = -1;
+	if (b->gpu_light_pending) {
+		// the host-built light nodes, then the root's device-built tree
+		const int n = (int)(b->gpu_light_elems.size() / 11);
+		const size_t host_nodes = b->light_nodes.size();
+		const size_t cap = host_nodes + 2 * (size_t)n - 1;
+		void* lp = nullptr;
+		if ((rc = ctx_cuda(ctx, cudaMalloc(&lp, cap * sizeof(DevLightNode)), "cudaMalloc(light_nodes)"))) return rc;
+		ctx->scene_allocs.push_back(lp);
+		ctx->device_bytes += cap * sizeof(DevLightNode);
+		if (host_nodes && (rc = ctx_cuda(ctx, cudaMemcpy(lp, b->light_nodes.data(), host_nodes * sizeof(DevLightNode),
+		                                                 cudaMemcpyHostToDevice), "cudaMemcpy(light_nodes)")))
+			return rc;
+		float energy = 0.0f;
+		if ((rc = ctx_cuda(ctx, build_light_tree_gpu(b->gpu_light_elems.data(), n, (int)host_nodes,
+		                                             (int)(b->light_extra.size() / 6),
+		                                             static_cast<DevLightNode*>(lp) + host_nodes, &energy, nullptr),
+		                   "psy_scene_upload_ex: device light tree build")))
+			return rc;
+		b->assemblies[0].light_root = (int)host_nodes;
+		b->assemblies[0].light_energy = energy;
+		ctx->gpu_light_nodes = 2 * n - 1;
+		d.light_nodes = static_cast<const DevLightNode*>(lp);
+	} else {
+		UP(light_nodes, b->light_nodes);
+	}
 	UP(assemblies, b->assemblies);
 	UP(instances, b->instances);
 	UP(objects, b->objects);
 	UP(node_extra, b->node_extra);
 	UP(xforms, b->xforms);
 	UP(fpool, b->fpool);
-	UP(light_nodes, b->light_nodes);
 	UP(light_extra, b->light_extra);
 	UP(shaders, b->shaders);
 	UP(cam_xforms, b->cam_xforms);
@@ -612,6 +637,7 @@ int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags
 	UP(cam_focus, b->cam_focus);
 #undef UP
 	d.assembly_count = (int)b->assemblies.size();
+	d.light_node_count = (int)b->light_nodes.size() + (ctx->gpu_light_nodes > 0 ? ctx->gpu_light_nodes : 0);
 	d.rcp = ctx->rcp;
 	d.max_depth = b->max_depth;
 	d.features = b->features;
@@ -638,9 +664,12 @@ int psy_scene_stats_get(const psy_ctx* ctx, psy_scene_stats* out) {
 	out->instances = (uint32_t)ctx->host->instances.size();
 	out->objects = (uint32_t)ctx->host->objects.size();
 	out->bvh4_nodes = (uint32_t)ctx->host->nodes.size() + (uint32_t)(ctx->gpu_bvh_nodes > 0 ? ctx->gpu_bvh_nodes : 0);
-	out->light_nodes = (uint32_t)ctx->host->light_nodes.size();
+	out->light_nodes =
+	    (uint32_t)ctx->host->light_nodes.size() + (uint32_t)(ctx->gpu_light_nodes > 0 ? ctx->gpu_light_nodes : 0);
 	out->lights = ctx->host->total_lights;
 	out->device_bytes = ctx->device_bytes;
+	out->gpu_bvh4_nodes = (uint32_t)(ctx->gpu_bvh_nodes > 0 ? ctx->gpu_bvh_nodes : 0);
+	out->gpu_light_nodes = (uint32_t)(ctx->gpu_light_nodes > 0 ? ctx->gpu_light_nodes : 0);
 	return PSY_OK;
 }
 

@@ -55,6 +55,7 @@ struct psy_ctx {
 	const unsigned long long* last_counts = nullptr;
 	// BVH4 nodes the last upload built on the device (-1: built on the host)
 	int gpu_bvh_nodes = -1;
+	int gpu_light_nodes = -1;  // light nodes the device built for the root, -1 if none
 
 	~psy_ctx();
 	void free_scene();

@@ -144,7 +144,7 @@ struct DevScene {
 	const float* cam_focus;
 	int cam_xform_count, cam_tfov_count, cam_aperture_count, cam_focus_count;
 	float background[3];
-	float pad0;
+	int light_node_count;  // all assemblies' light nodes (bounds a tree walk)
 	// the host CPU's approximate reciprocal (psy_math.h), for matrix inverses
 	RcpTable rcp;
 };

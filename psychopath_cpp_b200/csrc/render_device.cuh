@@ -750,7 +750,9 @@ static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, floa
 		if (as.light_root < 0) return;
 		int node = as.light_root;
 		float tot_prob = 1.0f;
-		for (int guard = 0; guard < 64; ++guard) {
+		// a tree is never deeper than its node count: the bound only stops a
+		// walk over a malformed tree
+		for (int guard = 0; guard < sc.light_node_count; ++guard) {
 			const DevLightNode nd = sc.light_nodes[node];
 			if (nd.is_leaf) break;
 			float p1 = light_node_prob(sc, *q, nd.c1);
@@ -774,7 +776,7 @@ static __device__ void light_tree_sample(const DevScene& sc, LightQuery* q, floa
 			}
 		}
 		const DevLightNode leaf = sc.light_nodes[node];
-		if (!leaf.is_leaf || leaf.c1 < 0 || leaf.c1 >= as.inst_count) return;  // deeper than the guard: no sample
+		if (!leaf.is_leaf || leaf.c1 < 0 || leaf.c1 >= as.inst_count) return;  // malformed tree: no sample
 		const int local = leaf.c1;
 		const DevInstance inst = sc.instances[as.inst_base + local];
 		q->id = id_push(q->id, (uint64_t)local, as.id_bits);

@@ -742,9 +742,10 @@ struct Builder {
 		return me;
 	}
 
-	void build_light_tree(HAssembly& ha, int aidx) {
-		std::vector<LBuild> bn;
-		uint32_t total_lights = 0;
+	// The assembly's lights as LightTree::build lists them (light_tree.cpp:
+	// 99-150): emitting object instances and assembly instances with lights.
+	void collect_lights(HAssembly& ha, std::vector<LBuild>& bn, uint32_t& total_lights) {
+		total_lights = 0;
 		for (uint32_t i = 0; i < ha.d->instance_count; ++i) {
 			const psy_instance_desc& id = ha.d->instances[i];
 			if (id.kind == PSY_INSTANCE_OBJECT) {
@@ -785,6 +786,12 @@ struct Builder {
 				}
 			}
 		}
+	}
+
+	void build_light_tree(HAssembly& ha, int aidx) {
+		std::vector<LBuild> bn;
+		uint32_t total_lights = 0;
+		collect_lights(ha, bn, total_lights);
 		DevAssembly& da = out->assemblies[aidx];
 		da.light_root = -1;
 		da.light_count = (int)total_lights;
@@ -822,6 +829,40 @@ struct Builder {
 		}
 	}
 
+	// The lights of the root for the device build of its light tree, when
+	// it has two or more and each light's bounds have one time sample
+	// (every node then has one box); false otherwise.
+	bool light_tree_for_gpu(HAssembly& ha, int aidx) {
+		std::vector<LBuild> bn;
+		uint32_t total_lights = 0;
+		collect_lights(ha, bn, total_lights);
+		if (bn.size() < 2) return false;
+		std::vector<float> el;
+		el.reserve(bn.size() * 11);
+		for (const LBuild& l : bn) {
+			const psy_instance_desc& id = ha.d->instances[l.instance];
+			std::vector<Box> bb;
+			if (id.kind == PSY_INSTANCE_OBJECT) {
+				bb = instance_bounds(ha, (uint32_t)l.instance);
+			} else {
+				const HAssembly& sub = asms[ha.children[id.data_index]];
+				bb = id.transform_count > 0 ? transform_from(sub.light_bounds, ha.xforms.data() + id.transform_index,
+				                                             (int)id.transform_count)
+				                            : sub.light_bounds;
+			}
+			if (bb.size() != 1 || l.instance >= (1u << 24)) return false;
+			el.insert(el.end(), {l.center.x, l.center.y, l.center.z, l.energy, (float)l.instance, bb[0].lo.x,
+			                     bb[0].lo.y, bb[0].lo.z, bb[0].hi.x, bb[0].hi.y, bb[0].hi.z});
+		}
+		out->gpu_light_elems.swap(el);
+		out->gpu_light_pending = true;
+		DevAssembly& da = out->assemblies[aidx];
+		da.light_root = -1;  // set by the device build
+		da.light_count = (int)total_lights;
+		ha.light_count = total_lights;
+		return true;
+	}
+
 	// ---------------------------------------------------------------
 	// The root's leaf boxes for the device build, when every root instance
 	// has a single bounding box; false otherwise.
@@ -846,14 +887,18 @@ struct Builder {
 		// the root is never instanced, so its reference-form tree (which gives
 		// an assembly its bounds) is not needed when the device builds its
 		// traversal tree
+		// the root's light tree is left to the device build when asked for
+		// and possible (the root is never instanced: nothing above it needs
+		// its light bounds)
+		const bool gpu_lights = a == 0 && gpu_root_bvh && light_tree_for_gpu(ha, a);
 		if (a == 0 && gpu_root_bvh && root_leaves_for_gpu(ha)) {
-			build_light_tree(ha, a);
+			if (!gpu_lights) build_light_tree(ha, a);
 			ha.finalized = true;
 			return maxd;
 		}
 		build_bvh4(ha, a, false);
 		build_bvh4(ha, a, true);
-		build_light_tree(ha, a);
+		if (!gpu_lights) build_light_tree(ha, a);
 		ha.finalized = true;
 		return maxd;
 	}

@@ -47,11 +47,19 @@ struct BuiltScene {
 	// assemblies[0].root stays REF_EMPTY until that build sets it.
 	bool gpu_root_pending = false;
 	std::vector<float> gpu_leaf_boxes;  // per root instance: lo xyz, hi xyz
+	// With gpu_root_bvh requested and a root with two or more lights whose
+	// bounds have one time sample each, the root's light tree is left to the
+	// device build: its lights in LightTree::build's order, 11 floats each
+	// (centre xyz, energy, local instance index, bounds lo xyz, hi xyz), and
+	// assemblies[0].light_root stays -1 until that build sets it.
+	bool gpu_light_pending = false;
+	std::vector<float> gpu_light_elems;
 };
 
 // Validates the description and builds every assembly (children first).
-// gpu_root_bvh: leave the root assembly's traversal tree to the device
-// build when it has no motion (see gpu_root_pending).  Returns PSY_OK or
+// gpu_root_bvh: leave the root assembly's traversal tree and light tree to
+// the device builds when they have no motion (see gpu_root_pending and
+// gpu_light_pending).  Returns PSY_OK or
 // PSY_ERR_ARG with *err set.
 int build_scene(const psy_scene_desc* desc, BuiltScene* out, std::string* err, bool gpu_root_bvh = false);
 

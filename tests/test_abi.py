@@ -51,3 +51,39 @@ def test_context_creation_without_a_device_fails_cleanly():
     h = C.c_void_p()
     assert L.psy_ctx_create(0, C.byref(h)) == _abi.PSY_ERR_DEVICE
     assert not h.value
+
+
+# ctypes mirror -> the header's struct it mirrors
+_MIRRORS = {
+    "ObjectDesc": "psy_object_desc", "InstanceDesc": "psy_instance_desc", "AssemblyDesc": "psy_assembly_desc",
+    "ShaderDesc": "psy_shader_desc", "SceneDesc": "psy_scene_desc", "SceneStats": "psy_scene_stats",
+    "RaySoA": "psy_ray_soa", "HitSoA": "psy_hit_soa", "LightQuerySoA": "psy_light_query_soa",
+    "LightSampleSoA": "psy_light_sample_soa", "RenderDesc": "psy_render_desc", "DiffDesc": "psy_diff_desc",
+    "BatchDesc": "psy_batch_desc", "BatchTuning": "psy_batch_tuning", "RenderStats": "psy_render_stats",
+    "TraceCounters": "psy_trace_counters",
+}
+
+
+def test_ctypes_mirrors_match_the_header_layout(tmp_path):
+    """Every ctypes structure has the size and field offsets that a C
+    compiler gives the header's struct of the same field names."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "psy_b200.h"', "int main(void) {"]
+    expect = []
+    for py, cn in _MIRRORS.items():
+        cls = getattr(_abi, py)
+        lines.append('printf("%%zu\\n", sizeof(%s));' % cn)
+        expect.append(C.sizeof(cls))
+        for f in cls._fields_:
+            lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (cn, f[0]))
+            expect.append(getattr(cls, f[0]).offset)
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == expect

@@ -55,12 +55,31 @@ def _light_queries(n, lo, hi, seed):
     return q
 
 
-@pytest.mark.parametrize("which", ["plain", "many", "bench"])
+def _stacked_light_scene(n_lights, seed):
+    """Lights on a few shared centres (and one axis), so that most splits
+    leave one part empty and take one light alone: trees as deep as their
+    light count, met by the one-warp splits too."""
+    from psychopath_cpp_b200.scene import SphereLight
+    sc = scenes.plain_scene(4)
+    rng = np.random.default_rng(seed)
+    spots = [[0.0, 0.0, 4.0], [0.0, 0.0, 5.0], [2.0, 1.0, 4.5], [-3.0, 0.5, 3.0], [2.0, 1.0, 4.5]]
+    for k in range(n_lights):
+        p = spots[int(rng.integers(len(spots)))]
+        sc.root.add_object("sl%d" % k, SphereLight([p], [0.1], [[float(rng.uniform(1, 50))] * 3]))
+        sc.root.add_instance("sl%d" % k)
+    return sc
+
+
+@pytest.mark.parametrize("which", ["plain", "many", "bench", "stacked"])
 def test_light_tree_sample_parity(ctx, ref_available, which):
     """LightTree::sample; "bench" is the 720p benchmark scene's own tree
-    (10,000 sphere lights, 19,999 nodes) with queries over its ground."""
+    (10,000 sphere lights, 19,999 nodes) with queries over its ground;
+    "stacked" a tree hundreds of levels deep (lights on shared centres)."""
     from oracle import psyref
-    if which == "plain":
+    if which == "stacked":
+        sc = _stacked_light_scene(400, 9)
+        q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 6), 4)
+    elif which == "plain":
         sc = scenes.plain_scene(4)
         q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 3), 1)
     elif which == "many":
@@ -79,6 +98,51 @@ def test_light_tree_sample_parity(ctx, ref_available, which):
                      ("light_pdf", slice(9, 10))):
         d = parity.ulp_diff(ref_out[:, sl], out[:, sl])
         assert d.max() == 0, (name, int((d > 0).sum()), int(d.max()))
+
+
+@pytest.mark.parametrize("which", ["plain", "rect", "many", "bench", "stacked"])
+def test_device_light_tree_matches_host(ctx, which):
+    """The root's light tree built on the device (upload with gpu_bvh) is
+    LightTree::build's tree node for node: every light choice and output bit
+    of LightTree::sample equal to the host-built tree's, over queries that
+    reach every part of the tree, and the same node count."""
+    if which == "stacked":
+        sc = _stacked_light_scene(400, 9)
+        q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 6), 4)
+    elif which == "plain":
+        sc = scenes.plain_scene(4)
+        q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 3), 1)
+    elif which == "rect":
+        sc = scenes.rect_light_scene(2)
+        q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 3), 3)
+    elif which == "many":
+        sc = scenes.many_light_scene(6, res=(64, 36), spp=1, n_patches=60, n_groups=30, n_lights=2000)
+        q = _light_queries(40000, (-8, -6, 0.0), (8, 6, 4), 2)
+    else:
+        sc = scenes.many_light_scene(3, res=(64, 36), spp=1)
+        q = _light_queries(100000, (-24, -19, 0.0), (24, 19, 8), 5)
+    ctx.upload(sc)
+    host = ctx.stats()
+    assert host["gpu_light_nodes"] == 0
+    a, ida = api.LightTree(ctx).sample(q)
+    ctx.upload(sc, gpu_bvh=True)
+    dev = ctx.stats()
+    assert dev["light_nodes"] == host["light_nodes"]
+    # the root's lights (one sphere in the plain scene: nothing to build)
+    n_root = {"plain": 0, "rect": 2, "many": 2000, "bench": 10000, "stacked": 401}[which]
+    assert dev["gpu_light_nodes"] == (2 * n_root - 1 if n_root > 1 else 0)
+    b, idb = api.LightTree(ctx).sample(q)
+    assert (ida == idb).all(), int((ida != idb).sum())
+    assert (a.view(np.uint32) == b.view(np.uint32)).all()
+    if which == "many":
+        # the root's traversal tree stays a host build here (its cluster
+        # instances move), so the images are the same bit for bit
+        sc = scenes.many_light_scene(7, res=(48, 27), spp=4, n_patches=80, n_groups=40, n_lights=500)
+        ctx.upload(sc)
+        x, _ = api.PathTraceIntegrator(ctx, 48, 27, 4, seed=1, path_length=4).integrate()
+        ctx.upload(sc, gpu_bvh=True)
+        y, _ = api.PathTraceIntegrator(ctx, 48, 27, 4, seed=1, path_length=4).integrate()
+        assert (np.asarray(x).view(np.uint32) == np.asarray(y).view(np.uint32)).all()
 
 
 def test_plain_render_matches_reference(ctx, ref_available):
