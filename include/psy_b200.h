@@ -145,10 +145,12 @@ int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* scene);
  * boxes, packed four-wide as BVH4::build packs, accel/bvh4.cpp:17-159),
  * when no root instance has motion (otherwise the host builds it as
  * psy_scene_upload does).  Hits are those of psy_scene_upload (exact ties
- * aside): only the tree that orders the candidates differs.  The light
- * tree and the nested assemblies' trees are built on the host either way
- * (the light tree's structure decides light selection, so it stays the
- * reference's).
+ * aside): only the tree that orders the candidates differs.  The root's
+ * light tree is built on the device too, when it has two or more lights
+ * whose bounds have no motion: LightTree::build's own tree node for node
+ * (accel/light_tree.cpp:99-238, libstdc++'s partition order included), so
+ * light selection is unchanged.  The nested assemblies' trees are built on
+ * the host either way.
  */
 #define PSY_UPLOAD_GPU_BVH 1u
 int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* scene, uint32_t flags);
