@@ -520,9 +520,20 @@ def run_batch_ours(args, rank, local, pg, world):
     torch.cuda.set_device(dev)
     cfgs = scenes.batch_configs(48, seed=0)
     ctxs, entries = [], []
+    # scene build and upload, the root's BVH4 and light tree built on the
+    # device against the host build (library call only, the fastest of two
+    # per scene); the renders below use the host build, whose SAH tree
+    # traverses faster than the device's linear BVH
+    build = {"device_s": 0.0, "host_s": 0.0, "device_bvh4_nodes": 0, "device_light_nodes": 0}
     for c in cfgs:
         ctx = api.Context(local)
-        ctx.upload(scenes.batch_scene(c["seed"], c["res"], c["spp"], c["n_prims"], c["n_lights"]))
+        flat = api.flatten(scenes.batch_scene(c["seed"], c["res"], c["spp"], c["n_prims"], c["n_lights"]))
+        build["device_s"] += min(ctx.upload_flat(flat, gpu_bvh=True) for _ in range(2))
+        st = ctx.stats()
+        build["device_bvh4_nodes"] += st["gpu_bvh4_nodes"]
+        build["device_light_nodes"] += st["gpu_light_nodes"]
+        build["host_s"] += min(ctx.upload_flat(flat) for _ in range(2))
+        del flat
         ctxs.append(ctx)
         entries.append({"scene": ctx, "width": c["res"][0], "height": c["res"][1], "spp": c["spp"],
                         "seed": c["seed"] + 1, "path_length": 4})
@@ -594,6 +605,13 @@ def run_batch_ours(args, rank, local, pg, world):
         "plain_paths_per_s": round(plain_value, 1), "plain_ms_per_step": round(plain_ms, 3),
         "plain_per_render": {"ms": [round(x, 3) for x in per_render_ms], "paths": per_render_paths},
         "batched_over_plain": round(value / plain_value, 3), "mrays_per_s": round(rays / (batch_ms * 1e-3) / 1e6, 2),
+        "scene_build": {"scenes": len(cfgs), "host_s": round(build["host_s"], 4),
+                        "device_s": round(build["device_s"], 4),
+                        "device_bvh4_nodes": build["device_bvh4_nodes"],
+                        "device_light_nodes": build["device_light_nodes"],
+                        "basis": "psy_scene_upload vs psy_scene_upload_ex(PSY_UPLOAD_GPU_BVH) per scene, "
+                                 "library call (scene build and copies to the device, the Python flattening "
+                                 "left out), fastest of 2"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 5), "traffic": None, "peak_source": peak_kind,
                      "basis": "R*80 + 20 B per path (R = rays per path)"},
@@ -857,7 +875,7 @@ def render_line_extras(args, rank, local, pg, world) -> dict:
     b = run_batch_ours(small, rank, local, pg, world)
     out["batched_over_plain"] = {"value": b["batched_over_plain"], "batched_paths_per_s": b["value"],
                                  "plain_paths_per_s": b["plain_paths_per_s"], "workload": b["config"]["workload"],
-                                 "steps": 1, "clocks": b["clocks"]}
+                                 "steps": 1, "clocks": b["clocks"], "scene_build": b["scene_build"]}
     out["batched_over_plain"]["small_renders"] = run_batch_small(local)
     small.steps, small.warmup = 10, 3
     a = run_adjoint_ours(small, rank, local, pg, world)

@@ -13,6 +13,7 @@ Every call goes through libpsy_b200.so; a missing library raises.
 from __future__ import annotations
 
 import ctypes as C
+import time
 from typing import Dict, List, Optional, Tuple
 
 import numpy as np
@@ -174,16 +175,25 @@ class Context:
         if rc != 0:
             raise _abi.PsyError(rc, self.L.psy_last_error(self.h).decode())
 
-    def upload(self, scene: Scene, gpu_bvh: bool = False) -> None:
-        """psy_scene_upload; gpu_bvh builds the root's traversal BVH4 on the
-        device (psy_scene_upload_ex with PSY_UPLOAD_GPU_BVH)."""
-        desc, keep = flatten(scene)
+    def upload(self, scene: Scene, gpu_bvh: bool = False) -> float:
+        """psy_scene_upload; gpu_bvh builds the root's traversal BVH4 and light
+        tree on the device (psy_scene_upload_ex with PSY_UPLOAD_GPU_BVH).
+        Returns the seconds spent in the library call (scene build and copy
+        to the device, without this module's flattening of `scene`)."""
+        dt = self.upload_flat(flatten(scene), gpu_bvh)
+        self.scene = scene
+        return dt
+
+    def upload_flat(self, flat, gpu_bvh: bool = False) -> float:
+        """upload() of a scene already flattened (flatten(scene)), for a scene
+        uploaded more than once; returns the library call's seconds."""
+        desc, _keep = flat
+        t0 = time.perf_counter()
         if gpu_bvh:
             self.check(self.L.psy_scene_upload_ex(self.h, C.byref(desc), _abi.PSY_UPLOAD_GPU_BVH))
         else:
             self.check(self.L.psy_scene_upload(self.h, C.byref(desc)))
-        del keep
-        self.scene = scene
+        return time.perf_counter() - t0
 
     def stats(self) -> dict:
         s = _abi.SceneStats()
