@@ -163,8 +163,8 @@ cudaError_t launch_trace(const DevScene& sc, const RaySoA& rays, const HitSoA& h
 // hi xyz; leaf k is local instance k).  The nodes go to d_nodes[0..] (room
 // for n - 1), numbered from node_base in their child references; *root_ref
 // and *node_count describe the result.  Synchronous on `st` (bvh_gpu.cu).
-cudaError_t build_bvh4_gpu(const float* h_boxes, int n, int node_base, DevNode* d_nodes, int* root_ref,
-                           int* node_count, cudaStream_t st);
+cudaError_t build_bvh4_gpu(const float* h_boxes, const float* h_centres, int n, int node_base, DevNode* d_nodes,
+                           int* root_ref, int* node_count, cudaStream_t st);
 
 // Device build of a light tree over n lights (host, 11 floats each, see
 // BuiltScene::gpu_light_elems) into d_nodes[0 .. 2n - 2], numbered from

@@ -117,7 +117,9 @@ __device__ void thread_split(const BuildOut& o, const Seg& s, LightElem* el) {
 		el[last] = t;
 		++first;
 	}
-	write_inner(o, s, first == s.start ? first + 1 : first);
+	// (every light in front of the plane only when it overflowed to infinity:
+	// both parts non-empty all the same)
+	write_inner(o, s, first == s.start ? first + 1 : (first == s.end ? first - 1 : first));
 }
 
 // The same split by one warp.  The two-ended loop's outcome in closed form:
@@ -183,7 +185,7 @@ __device__ void warp_split(const BuildOut& o, const Seg& s, LightElem* el, int* 
 		r += __popc(b);
 	}
 	__syncwarp();
-	if (lane == 0) write_inner(o, s, midp == s.start ? midp + 1 : midp);
+	if (lane == 0) write_inner(o, s, midp == s.start ? midp + 1 : (midp == s.end ? midp - 1 : midp));
 	__syncwarp();
 }
 

@@ -587,7 +587,7 @@ int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags
 		                                                 cudaMemcpyHostToDevice), "cudaMemcpy(nodes)")))
 			return rc;
 		int root = REF_EMPTY, count = 0;
-		if ((rc = ctx_cuda(ctx, build_bvh4_gpu(b->gpu_leaf_boxes.data(), n, (int)host_nodes,
+		if ((rc = ctx_cuda(ctx, build_bvh4_gpu(b->gpu_leaf_boxes.data(), b->gpu_leaf_centres.data(), n, (int)host_nodes,
 		                                       static_cast<DevNode*>(np) + host_nodes, &root, &count, nullptr),
 		                   "psy_scene_upload_ex: device BVH build")))
 			return rc;

@@ -46,7 +46,8 @@ struct BuiltScene {
 	// to the device build: its leaf boxes are here, in instance order, and
 	// assemblies[0].root stays REF_EMPTY until that build sets it.
 	bool gpu_root_pending = false;
-	std::vector<float> gpu_leaf_boxes;  // per root instance: lo xyz, hi xyz
+	std::vector<float> gpu_leaf_boxes;    // per root instance: lo xyz, hi xyz
+	std::vector<float> gpu_leaf_centres;  // per root instance: its box's centre at time 0.5
 	// With gpu_root_bvh requested and a root with two or more lights whose
 	// bounds have one time sample each, the root's light tree is left to the
 	// device build: its lights in LightTree::build's order, 11 floats each
