@@ -393,27 +393,59 @@ __global__ void __launch_bounds__(kBlock, 1) sah_build_kernel(SahElem* __restric
 	}
 }
 
-__global__ void bounds_kernel(const unsigned long long* __restrict__ keys, const float* __restrict__ boxes, int n,
-                              int root, const int* __restrict__ left, const int* __restrict__ right,
-                              const int* __restrict__ parent, int* __restrict__ arrived, float* nbox) {
+// A node's time sample i: nbox holds max_ts samples per node.
+__device__ __forceinline__ Box node_box(const float* nbox, int max_ts, int node, int i) {
+	const volatile float* b = nbox + ((size_t)node * max_ts + i) * 6;
+	Box r;
+	r.lo = V3(b[0], b[1], b[2]);
+	r.hi = V3(b[3], b[4], b[5]);
+	return r;
+}
+
+__device__ __forceinline__ void put_box(float* nbox, int max_ts, int node, int i, const Box& x) {
+	float* b = nbox + ((size_t)node * max_ts + i) * 6;
+	b[0] = x.lo.x; b[1] = x.lo.y; b[2] = x.lo.z;
+	b[3] = x.hi.x; b[4] = x.hi.y; b[5] = x.hi.z;
+}
+
+// Node boxes bottom-up, with the host builder's time-sample rule: children
+// with as many samples give their per-sample unions, children with
+// different counts one box over all of their samples.
+__global__ void bounds_kernel(const unsigned long long* __restrict__ keys, const float* __restrict__ samples,
+                              const int* __restrict__ first, int n, int max_ts, int root,
+                              const int* __restrict__ left, const int* __restrict__ right,
+                              const int* __restrict__ parent, int* __restrict__ arrived, int* nts, float* nbox) {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= n) return;
 	const int inst = (int)(keys[k] & 0xffffffffull);
 	int node = (n - 1) + k;
-	for (int c = 0; c < 6; ++c) nbox[6 * (size_t)node + c] = boxes[6 * (size_t)inst + c];
+	const int ts = first[inst + 1] - first[inst];
+	for (int i = 0; i < ts; ++i) {
+		const float* s = samples + 6 * (size_t)(first[inst] + i);
+		Box x;
+		x.lo = V3(s[0], s[1], s[2]);
+		x.hi = V3(s[3], s[4], s[5]);
+		put_box(nbox, max_ts, node, i, x);
+	}
+	nts[node] = ts;
 	while (node != root) {
 		__threadfence();
 		const int p = parent[node];
 		if (atomicAdd(&arrived[p], 1) == 0) return;  // the other child is not done yet
 		__threadfence();
-		const volatile float* a = nbox + 6 * (size_t)left[p];
-		const volatile float* b = nbox + 6 * (size_t)right[p];
-		float u[6];
-		for (int c = 0; c < 3; ++c) {
-			u[c] = fminf(a[c], b[c]);
-			u[3 + c] = fmaxf(a[3 + c], b[3 + c]);
+		const int a = left[p], b = right[p];
+		const int ta = ((const volatile int*)nts)[a], tb = ((const volatile int*)nts)[b];
+		if (ta == tb) {
+			for (int i = 0; i < ta; ++i)
+				put_box(nbox, max_ts, p, i, box_union(node_box(nbox, max_ts, a, i), node_box(nbox, max_ts, b, i)));
+			nts[p] = ta;
+		} else {
+			Box m = node_box(nbox, max_ts, a, 0);
+			for (int i = 1; i < ta; ++i) m = box_union(m, node_box(nbox, max_ts, a, i));
+			for (int i = 0; i < tb; ++i) m = box_union(m, node_box(nbox, max_ts, b, i));
+			put_box(nbox, max_ts, p, 0, m);
+			nts[p] = 1;
 		}
-		for (int c = 0; c < 6; ++c) nbox[6 * (size_t)p + c] = u[c];
 		node = p;
 	}
 }
@@ -421,11 +453,17 @@ __global__ void bounds_kernel(const unsigned long long* __restrict__ keys, const
 // One level of BVH4 nodes: each queued binary inner node becomes a device
 // node whose children are its binary children, or their children when they
 // are inner nodes; inner children are numbered and queued for the next level.
+// A node's time samples are its children's when they have as many, else as
+// many as the most of them, the others' boxes interpolated at each sample's
+// time (BVH4::build, accel/bvh4.cpp:88-135); samples after the first go to
+// the extra records.
 __global__ void collapse_kernel(const int* __restrict__ queue_in, int n_in, const int* __restrict__ index_in,
                                 int* __restrict__ queue_out, int* __restrict__ index_out, int* __restrict__ n_out,
                                 int* __restrict__ counter, const unsigned long long* __restrict__ keys, int n,
                                 const int* __restrict__ left, const int* __restrict__ right,
-                                const float* __restrict__ nbox, int node_base, DevNode* __restrict__ nodes) {
+                                const int* __restrict__ nts, const float* __restrict__ nbox, int max_ts,
+                                int node_base, DevNode* __restrict__ nodes, float* __restrict__ extra,
+                                int* __restrict__ extra_count, int extra_base) {
 	const int q = blockIdx.x * blockDim.x + threadIdx.x;
 	if (q >= n_in) return;
 	const int bn = queue_in[q];
@@ -442,12 +480,41 @@ __global__ void collapse_kernel(const int* __restrict__ queue_in, int n_in, cons
 		}
 	}
 	DevNode dn;
+	bool equal_ts = true;
+	int most = nts[kids[0]];
+	for (int c = 1; c < nk; ++c) {
+		equal_ts = equal_ts && nts[kids[c - 1]] == nts[kids[c]];
+		most = nts[kids[c]] > most ? nts[kids[c]] : most;
+	}
+	const int rts = equal_ts ? nts[kids[0]] : most;
+	const int ex = rts > 1 ? atomicAdd(extra_count, rts - 1) : 0;
+	for (int i = 0; i < rts; ++i) {
+		float* rec = i == 0 ? dn.b : extra + (size_t)(ex + i - 1) * 24;
+		for (int c = 0; c < 4; ++c) {
+			Box x = box_empty();
+			if (c < nk) {
+				const int kc = kids[c], tc = nts[kc];
+				if (equal_ts || tc == most) {
+					x = node_box(nbox, max_ts, kc, i);
+				} else {
+					const SeqPos sp = seq_pos((float)i / (float)(most - 1), tc);
+					x = sp.single ? node_box(nbox, max_ts, kc, sp.i0)
+					              : box_lerp(sp.nalpha, node_box(nbox, max_ts, kc, sp.i0),
+					                         node_box(nbox, max_ts, kc, sp.i0 + 1));
+				}
+			}
+			rec[0 * 4 + c] = x.lo.x;
+			rec[1 * 4 + c] = x.hi.x;
+			rec[2 * 4 + c] = x.lo.y;
+			rec[3 * 4 + c] = x.hi.y;
+			rec[4 * 4 + c] = x.lo.z;
+			rec[5 * 4 + c] = x.hi.z;
+		}
+	}
 	for (int c = 0; c < 4; ++c) {
-		float b[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
 		int ref = REF_EMPTY;
 		if (c < nk) {
 			const int x = kids[c];
-			for (int k = 0; k < 6; ++k) b[k] = nbox[6 * (size_t)x + k];
 			if (x >= n - 1) {
 				ref = leaf_ref((int)(keys[x - (n - 1)] & 0xffffffffull));
 			} else {
@@ -458,17 +525,11 @@ __global__ void collapse_kernel(const int* __restrict__ queue_in, int n_in, cons
 				ref = node_base + idx;
 			}
 		}
-		dn.b[0 * 4 + c] = b[0];
-		dn.b[1 * 4 + c] = b[3];
-		dn.b[2 * 4 + c] = b[1];
-		dn.b[3 * 4 + c] = b[4];
-		dn.b[4 * 4 + c] = b[2];
-		dn.b[5 * 4 + c] = b[5];
 		dn.child[c] = ref;
 	}
 	dn.nchild = nk;
-	dn.ts = 1;
-	dn.extra = 0;
+	dn.ts = rts;
+	dn.extra = rts > 1 ? extra_base + ex : 0;
 	dn.pad = 0;
 	nodes[index_in[q]] = dn;
 }
@@ -496,9 +557,11 @@ struct Scratch {
 
 }  // namespace
 
-cudaError_t build_bvh4_gpu(const float* h_boxes, const float* h_centres, int n, int node_base, DevNode* d_nodes,
-                           int* root_ref, int* node_count, cudaStream_t st) {
+cudaError_t build_bvh4_gpu(const float* h_samples, const int* h_first, const float* h_centres, int n,
+                           int node_base, DevNode* d_nodes, float* d_extra, int extra_base, int* root_ref,
+                           int* node_count, int* extra_count, cudaStream_t st) {
 	*node_count = 0;
+	*extra_count = 0;
 	if (n == 0) {
 		*root_ref = REF_EMPTY;
 		return cudaSuccess;
@@ -507,19 +570,40 @@ cudaError_t build_bvh4_gpu(const float* h_boxes, const float* h_centres, int n, 
 		*root_ref = leaf_ref(0);
 		return cudaSuccess;
 	}
+	// the surface-area split bins each instance's box over all its samples
 	std::vector<SahElem> el((size_t)n);
-	for (int i = 0; i < n; ++i)
+	std::vector<float> ubox(6 * (size_t)n);
+	int max_ts = 1;
+	for (int i = 0; i < n; ++i) {
 		el[i] = SahElem{{h_centres[3 * (size_t)i], h_centres[3 * (size_t)i + 1], h_centres[3 * (size_t)i + 2]}, i};
+		const int ts = h_first[i + 1] - h_first[i];
+		if (ts < 1) return cudaErrorInvalidValue;
+		max_ts = ts > max_ts ? ts : max_ts;
+		Box u = box_empty();
+		for (int k = 0; k < ts; ++k) {
+			const float* s = h_samples + 6 * (size_t)(h_first[i] + k);
+			Box x;
+			x.lo = V3(s[0], s[1], s[2]);
+			x.hi = V3(s[3], s[4], s[5]);
+			u = box_union(u, x);
+		}
+		const float f[6] = {u.lo.x, u.lo.y, u.lo.z, u.hi.x, u.hi.y, u.hi.z};
+		for (int c = 0; c < 6; ++c) ubox[6 * (size_t)i + c] = f[c];
+	}
+	const size_t n_samples = (size_t)h_first[n];
 	Scratch s;
 	SahElem* d_el;
 	Seg* d_seg;
-	float *d_boxes, *d_nbox;
+	float *d_ubox, *d_samples, *d_nbox;
 	unsigned long long* d_keys;
-	int *d_left, *d_right, *d_parent, *d_arrived, *d_pos, *d_q[2], *d_idx[2], *d_count;
+	int *d_first, *d_nts, *d_left, *d_right, *d_parent, *d_arrived, *d_pos, *d_q[2], *d_idx[2], *d_count;
 	PSY_TRY(s.get(&d_el, n));
 	PSY_TRY(s.get(&d_seg, 2 * (size_t)n - 1));
-	PSY_TRY(s.get(&d_boxes, 6 * (size_t)n));
-	PSY_TRY(s.get(&d_nbox, 6 * (size_t)(2 * n - 1)));
+	PSY_TRY(s.get(&d_ubox, 6 * (size_t)n));
+	PSY_TRY(s.get(&d_samples, 6 * n_samples));
+	PSY_TRY(s.get(&d_first, (size_t)n + 1));
+	PSY_TRY(s.get(&d_nbox, 6 * (size_t)max_ts * (size_t)(2 * n - 1)));
+	PSY_TRY(s.get(&d_nts, 2 * (size_t)n - 1));
 	PSY_TRY(s.get(&d_keys, n));
 	PSY_TRY(s.get(&d_left, n - 1));
 	PSY_TRY(s.get(&d_right, n - 1));
@@ -530,20 +614,23 @@ cudaError_t build_bvh4_gpu(const float* h_boxes, const float* h_centres, int n, 
 	PSY_TRY(s.get(&d_q[1], n));
 	PSY_TRY(s.get(&d_idx[0], n));
 	PSY_TRY(s.get(&d_idx[1], n));
-	PSY_TRY(s.get(&d_count, 3));
+	PSY_TRY(s.get(&d_count, 4));
 	PSY_TRY(cudaMemcpyAsync(d_el, el.data(), sizeof(SahElem) * (size_t)n, cudaMemcpyHostToDevice, st));
-	PSY_TRY(cudaMemcpyAsync(d_boxes, h_boxes, 6 * sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st));
+	PSY_TRY(cudaMemcpyAsync(d_ubox, ubox.data(), sizeof(float) * ubox.size(), cudaMemcpyHostToDevice, st));
+	PSY_TRY(cudaMemcpyAsync(d_samples, h_samples, 6 * sizeof(float) * n_samples, cudaMemcpyHostToDevice, st));
+	PSY_TRY(cudaMemcpyAsync(d_first, h_first, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, st));
 	PSY_TRY(cudaMemsetAsync(d_arrived, 0, sizeof(int) * (size_t)(n - 1), st));
+	PSY_TRY(cudaMemsetAsync(d_count, 0, sizeof(int) * 4, st));
 	const SahOut o{d_left, d_right, d_parent, d_keys, d_count + 2, d_seg, nullptr};
-	sah_build_kernel<<<1, kBlock, 0, st>>>(d_el, d_boxes, n, o, d_pos);
+	sah_build_kernel<<<1, kBlock, 0, st>>>(d_el, d_ubox, n, o, d_pos);
 	PSY_TRY(cudaGetLastError());
 	int root = 0;
 	PSY_TRY(cudaMemcpyAsync(&root, d_count + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
 	PSY_TRY(cudaStreamSynchronize(st));
 	if (root < 0 || root >= n - 1) return cudaErrorUnknown;  // n >= 2: the root is an inner node
 	const int B = 256;
-	bounds_kernel<<<(n + B - 1) / B, B, 0, st>>>(d_keys, d_boxes, n, root, d_left, d_right, d_parent, d_arrived,
-	                                             d_nbox);
+	bounds_kernel<<<(n + B - 1) / B, B, 0, st>>>(d_keys, d_samples, d_first, n, max_ts, root, d_left, d_right,
+	                                             d_parent, d_arrived, d_nts, d_nbox);
 	PSY_TRY(cudaGetLastError());
 	// level by level from the root (device node 0)
 	const int zero_one[2] = {0, 1};
@@ -554,17 +641,19 @@ cudaError_t build_bvh4_gpu(const float* h_boxes, const float* h_centres, int n, 
 	while (n_in > 0) {
 		PSY_TRY(cudaMemsetAsync(d_count + 1, 0, sizeof(int), st));
 		collapse_kernel<<<(n_in + B - 1) / B, B, 0, st>>>(d_q[cur], n_in, d_idx[cur], d_q[1 - cur], d_idx[1 - cur],
-		                                                  d_count + 1, d_count, d_keys, n, d_left, d_right, d_nbox,
-		                                                  node_base, d_nodes);
+		                                                  d_count + 1, d_count, d_keys, n, d_left, d_right, d_nts,
+		                                                  d_nbox, max_ts, node_base, d_nodes, d_extra, d_count + 3,
+		                                                  extra_base);
 		PSY_TRY(cudaGetLastError());
 		PSY_TRY(cudaMemcpyAsync(&n_in, d_count + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
 		PSY_TRY(cudaStreamSynchronize(st));
 		cur = 1 - cur;
 	}
-	int total = 0;
-	PSY_TRY(cudaMemcpyAsync(&total, d_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+	int totals[4] = {0, 0, 0, 0};
+	PSY_TRY(cudaMemcpyAsync(totals, d_count, sizeof(totals), cudaMemcpyDeviceToHost, st));
 	PSY_TRY(cudaStreamSynchronize(st));
-	*node_count = total;
+	*node_count = totals[0];
+	*extra_count = totals[3];
 	*root_ref = node_base;
 	return cudaSuccess;
 }

@@ -159,12 +159,18 @@ cudaError_t launch_light_sample(const DevScene& sc, const LightQuerySoADev& q, c
 cudaError_t launch_trace(const DevScene& sc, const RaySoA& rays, const HitSoA& hits, uint32_t n, unsigned* status,
                          cudaStream_t stream);
 
-// Device build of a BVH4 over n leaf boxes (host, 6 floats each: lo xyz,
-// hi xyz; leaf k is local instance k).  The nodes go to d_nodes[0..] (room
-// for n - 1), numbered from node_base in their child references; *root_ref
-// and *node_count describe the result.  Synchronous on `st` (bvh_gpu.cu).
-cudaError_t build_bvh4_gpu(const float* h_boxes, const float* h_centres, int n, int node_base, DevNode* d_nodes,
-                           int* root_ref, int* node_count, cudaStream_t st);
+// Device build of a BVH4 over n leaves (leaf k is local instance k): host
+// arrays of every instance's time-sample boxes (6 floats each: lo xyz, hi
+// xyz; instance i's are samples [h_first[i], h_first[i + 1])) and box
+// centres at time 0.5 (3 floats each).  The nodes go to d_nodes[0..] (room
+// for n - 1), numbered from node_base in their child references; their
+// time samples after the first to d_extra (24 floats each, room for
+// (n - 1) * (most samples - 1)), numbered from extra_base.  *root_ref,
+// *node_count and *extra_count describe the result.  Synchronous on `st`
+// (bvh_gpu.cu).
+cudaError_t build_bvh4_gpu(const float* h_samples, const int* h_first, const float* h_centres, int n,
+                           int node_base, DevNode* d_nodes, float* d_extra, int extra_base, int* root_ref,
+                           int* node_count, int* extra_count, cudaStream_t st);
 
 // Device build of a light tree over n lights (host, 11 floats each, see
 // BuiltScene::gpu_light_elems) into d_nodes[0 .. 2n - 2], numbered from

@@ -576,7 +576,7 @@ int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags
 	ctx->gpu_bvh_nodes = -1;
 	if (b->gpu_root_pending) {
 		// the host-built nodes, then room for the root's device-built ones
-		const int n = (int)(b->gpu_leaf_boxes.size() / 6);
+		const int n = (int)b->gpu_leaf_first.size() - 1;
 		const size_t host_nodes = b->nodes.size();
 		const size_t cap = host_nodes + (size_t)(n > 1 ? n - 1 : 0);
 		void* np = nullptr;
@@ -586,16 +586,35 @@ int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags
 		if (host_nodes && (rc = ctx_cuda(ctx, cudaMemcpy(np, b->nodes.data(), host_nodes * sizeof(DevNode),
 		                                                 cudaMemcpyHostToDevice), "cudaMemcpy(nodes)")))
 			return rc;
-		int root = REF_EMPTY, count = 0;
-		if ((rc = ctx_cuda(ctx, build_bvh4_gpu(b->gpu_leaf_boxes.data(), b->gpu_leaf_centres.data(), n, (int)host_nodes,
-		                                       static_cast<DevNode*>(np) + host_nodes, &root, &count, nullptr),
+		// the host-built nodes' later time samples, then room for the device
+		// nodes' (at most one record per sample after the first)
+		int most = 1;
+		for (int i = 0; i < n; ++i) most = std::max(most, b->gpu_leaf_first[i + 1] - b->gpu_leaf_first[i]);
+		const size_t host_extra = b->node_extra.size();
+		const size_t extra_cap = host_extra + (size_t)(n > 1 ? n - 1 : 0) * (size_t)(most - 1) * 24;
+		void* ep = nullptr;
+		if ((rc = ctx_cuda(ctx, cudaMalloc(&ep, (extra_cap ? extra_cap : 1) * sizeof(float)), "cudaMalloc(node_extra)")))
+			return rc;
+		ctx->scene_allocs.push_back(ep);
+		ctx->device_bytes += extra_cap * sizeof(float);
+		if (host_extra && (rc = ctx_cuda(ctx, cudaMemcpy(ep, b->node_extra.data(), host_extra * sizeof(float),
+		                                                 cudaMemcpyHostToDevice), "cudaMemcpy(node_extra)")))
+			return rc;
+		int root = REF_EMPTY, count = 0, extras = 0;
+		if ((rc = ctx_cuda(ctx, build_bvh4_gpu(b->gpu_leaf_boxes.data(), b->gpu_leaf_first.data(),
+		                                       b->gpu_leaf_centres.data(), n, (int)host_nodes,
+		                                       static_cast<DevNode*>(np) + host_nodes,
+		                                       static_cast<float*>(ep) + host_extra, (int)(host_extra / 24), &root,
+		                                       &count, &extras, nullptr),
 		                   "psy_scene_upload_ex: device BVH build")))
 			return rc;
 		b->assemblies[0].root = root;
 		ctx->gpu_bvh_nodes = count;
 		d.nodes = static_cast<const DevNode*>(np);
+		d.node_extra = static_cast<const float*>(ep);
 	} else {
 		UP(nodes, b->nodes);
+		UP(node_extra, b->node_extra);
 	}
 	ctx->gpu_light_nodes = -1;
 	if (b->gpu_light_pending) {
@@ -626,7 +645,6 @@ int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags
 	UP(assemblies, b->assemblies);
 	UP(instances, b->instances);
 	UP(objects, b->objects);
-	UP(node_extra, b->node_extra);
 	UP(xforms, b->xforms);
 	UP(fpool, b->fpool);
 	UP(light_extra, b->light_extra);

@@ -864,21 +864,23 @@ struct Builder {
 	}
 
 	// ---------------------------------------------------------------
-	// The root's leaf boxes for the device build, when every root instance
-	// has a single bounding box; false otherwise.
+	// The root's leaf bounds for the device build (every time sample), when
+	// every root instance has bounds; false otherwise.
 	bool root_leaves_for_gpu(HAssembly& ha) {
 		std::vector<float> boxes, centres;
+		std::vector<int> first{0};
 		for (uint32_t i = 0; i < ha.d->instance_count; ++i) {
 			const std::vector<Box> bbs = instance_bounds(ha, i);
-			if (bbs.size() != 1) return false;
-			const Box& b = bbs[0];
-			boxes.insert(boxes.end(), {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z});
+			if (bbs.empty() || bbs.size() > 64) return false;
+			for (const Box& b : bbs) boxes.insert(boxes.end(), {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z});
+			first.push_back(first.back() + (int)bbs.size());
 			// the centre build_bvh4 splits on
 			const Box bh = instance_bounds_at(ha, 0.5f, i);
 			const V3 c = lerp3(0.5f, bh.lo, bh.hi);
 			centres.insert(centres.end(), {c.x, c.y, c.z});
 		}
 		out->gpu_leaf_boxes.swap(boxes);
+		out->gpu_leaf_first.swap(first);
 		out->gpu_leaf_centres.swap(centres);
 		out->gpu_root_pending = true;
 		out->assemblies[0].root = REF_EMPTY;

@@ -41,12 +41,13 @@ struct BuiltScene {
 	unsigned features = 0;  // FEAT_* present
 	uint32_t total_lights = 0;
 	std::vector<RefBVH4> ref_bvh4;    // per assembly
-	// With gpu_root_bvh requested and a root assembly whose instances all
-	// have one bounding box (no motion), the root's traversal BVH4 is left
-	// to the device build: its leaf boxes are here, in instance order, and
-	// assemblies[0].root stays REF_EMPTY until that build sets it.
+	// With gpu_root_bvh requested, the root's traversal BVH4 is left to the
+	// device build: its instances' bounds (every time sample) are here, in
+	// instance order, and assemblies[0].root stays REF_EMPTY until that
+	// build sets it.
 	bool gpu_root_pending = false;
-	std::vector<float> gpu_leaf_boxes;    // per root instance: lo xyz, hi xyz
+	std::vector<float> gpu_leaf_boxes;    // every root instance's time samples: lo xyz, hi xyz
+	std::vector<int> gpu_leaf_first;      // instance i's samples: [first[i], first[i + 1])
 	std::vector<float> gpu_leaf_centres;  // per root instance: its box's centre at time 0.5
 	// With gpu_root_bvh requested and a root with two or more lights whose
 	// bounds have one time sample each, the root's light tree is left to the
@@ -58,9 +59,9 @@ struct BuiltScene {
 };
 
 // Validates the description and builds every assembly (children first).
-// gpu_root_bvh: leave the root assembly's traversal tree and light tree to
-// the device builds when they have no motion (see gpu_root_pending and
-// gpu_light_pending).  Returns PSY_OK or
+// gpu_root_bvh: leave the root assembly's traversal tree and (when its
+// lights do not move) its light tree to the device builds (see
+// gpu_root_pending and gpu_light_pending).  Returns PSY_OK or
 // PSY_ERR_ARG with *err set.
 int build_scene(const psy_scene_desc* desc, BuiltScene* out, std::string* err, bool gpu_root_bvh = false);
 

@@ -190,17 +190,25 @@ def test_nan_differentials_end_at_min_upoly(ctx, ref_available):
         np.testing.assert_array_equal(mine_zero[k], mine_nan[k])
 
 
-@pytest.mark.parametrize("kind", ["batch", "heightfield"])
+@pytest.mark.parametrize("kind", ["batch", "heightfield", "motion", "motion_patch"])
 def test_device_built_bvh_gives_the_same_hits(ctx, ref_available, kind):
     """psy_scene_upload_ex(PSY_UPLOAD_GPU_BVH): the root's traversal BVH4
     built on the device.  It is the host's surface-area tree split for split,
     so the hits agree with the reference's, every output bit equals the
     host-built tree's, and a render visits the same nodes and gives the same
-    image bit for bit."""
+    image bit for bit.  "motion" and "motion_patch" have root instances
+    with two time samples (moving clusters of instanced spheres, moving
+    patches), so nodes carry time samples of their own."""
     from oracle import psyref
     if kind == "batch":
         sc = scenes.batch_scene(10, (64, 48), 4, 20000, 20)
         rays = parity.random_rays(60000, (-7, -7, -0.5), (7, 7, 4), seed=41, occl_frac=0.3, width=0.002)
+    elif kind == "motion":
+        sc = scenes.many_light_scene(7, res=(64, 48), spp=4, n_patches=80, n_groups=40, n_lights=500)
+        rays = parity.random_rays(60000, (-8, -6, 0.0), (8, 6, 4), seed=43, occl_frac=0.3, width=0.002)
+    elif kind == "motion_patch":
+        sc = scenes.motion_patch_scene(1, res=(64, 48), spp=4)
+        rays = parity.random_rays(60000, (-6, -6, -0.5), (6, 6, 4), seed=44, occl_frac=0.3, width=0.002)
     else:
         sc = scenes.heightfield_scene(64, seed=5)
         rays = scenes.heightfield_rays(60000, n=64, seed=42)
@@ -220,7 +228,7 @@ def test_device_built_bvh_gives_the_same_hits(ctx, ref_available, kind):
     for k in fields:
         np.testing.assert_array_equal(np.asarray(host_tree[k]).view(np.uint8), np.asarray(dev_tree[k]).view(np.uint8))
     assert st["gpu_bvh4_nodes"] > 0 and st["bvh4_nodes"] == host_st["bvh4_nodes"]
-    if kind != "batch":
+    if kind == "heightfield":
         return  # the heightfield scene has no light to render with
     work = ("rays", "node_visits", "leaf_visits", "patch_iterations")
     ctx.upload(sc)
