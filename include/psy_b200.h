@@ -140,11 +140,11 @@ int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* scene);
 /*
  * psy_scene_upload with options (no counterpart in the reference, whose
  * builds run on the host at Assembly::finalize).  PSY_UPLOAD_GPU_BVH: the
- * root assembly's traversal BVH4 is built on the device, when no root
- * instance has motion (otherwise the host builds it as psy_scene_upload
- * does): the host's binned surface-area tree split for split, packed
- * four-wide as BVH4::build packs (accel/bvh4.cpp:17-159), so traces and
- * renders are those of psy_scene_upload bit for bit.  The root's
+ * root assembly's traversal BVH4 is built on the device (moving instances
+ * included): the host's binned surface-area tree split for split, packed
+ * four-wide as BVH4::build packs (accel/bvh4.cpp:17-159, time samples
+ * included), so traces and renders are those of psy_scene_upload bit for
+ * bit.  The root's
  * light tree is built on the device too, when it has two or more lights
  * whose bounds have no motion: LightTree::build's own tree node for node
  * (accel/light_tree.cpp:99-238, libstdc++'s partition order included), so
