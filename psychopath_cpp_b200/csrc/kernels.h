@@ -172,13 +172,16 @@ cudaError_t build_bvh4_gpu(const float* h_samples, const int* h_first, const flo
                            int node_base, DevNode* d_nodes, float* d_extra, int extra_base, int* root_ref,
                            int* node_count, int* extra_count, cudaStream_t st);
 
-// Device build of a light tree over n lights (host, 11 floats each, see
-// BuiltScene::gpu_light_elems) into d_nodes[0 .. 2n - 2], numbered from
-// node_base in their child references, time-sample extra index `extra`;
-// *root_energy receives the root's energy.  Synchronous on `st`
-// (light_gpu.cu).
-cudaError_t build_light_tree_gpu(const float* h_elems, int n, int node_base, int extra, DevLightNode* d_nodes,
-                                 float* root_energy, cudaStream_t st);
+// Device build of a light tree over n lights (host arrays, see
+// BuiltScene::gpu_light_elems / gpu_light_samples / gpu_light_first) into
+// d_nodes[0 .. 2n - 2], numbered from node_base in their child references;
+// the nodes' bounds samples after the first go to d_extra (6 floats each,
+// room for (2n - 1) * (most samples - 1)), numbered from extra_base.
+// *root_energy and *extra_count receive the root's energy and the records
+// written.  Synchronous on `st` (light_gpu.cu).
+cudaError_t build_light_tree_gpu(const float* h_elems, const float* h_samples, const int* h_first, int n,
+                                 int node_base, DevLightNode* d_nodes, float* d_extra, int extra_base,
+                                 float* root_energy, int* extra_count, cudaStream_t st);
 
 }  // namespace psy
 

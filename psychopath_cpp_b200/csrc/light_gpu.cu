@@ -15,7 +15,10 @@
  *     n lights takes 2n - 1 nodes, its first part's subtree right after it,
  *     the second part's after that;
  *   - inner bounds and energies come bottom-up as unions and sums of the
- *     two children, in child order (light_tree.cpp:223-229).
+ *     two children, in child order (light_tree.cpp:223-229); bounds are
+ *     time-sample sequences, merged per sample when the children have as
+ *     many samples, else each of the longer sequence's samples with the
+ *     shorter sequence interpolated at its time.
  * The segments of one level are independent, so each level's splits run in
  * parallel: a segment of more than 32 lights is split by one warp, a smaller
  * one by one thread.  Every node's children are on the next level, so the
@@ -46,22 +49,76 @@ constexpr int kBlock = 1024;
 constexpr int kWarps = kBlock / 32;
 constexpr unsigned kFull = 0xffffffffu;
 
-struct BuildOut {
-	DevLightNode* nodes;
-	int base, extra;
-	Seg* segs;  // every level's segments, level after level (2n - 1 in all)
-	int* total; // segments written so far (shared memory)
+// Time samples of the bounds: the lights' (light i's are samples
+// [first[i], first[i + 1])), every node's while the tree is built (max_ts
+// per node), and the records of a node's samples after the first.
+struct LightSamples {
+	const float* samples;
+	const int* first;
+	float* nbuf;
+	int* nts;
+	int max_ts;
+	float* extra;       // 6 floats per record
+	int* extra_count;
+	int extra_base;     // record index of extra[0]
 };
 
-__device__ __forceinline__ void write_leaf(const BuildOut& o, const Seg& s, const LightElem* el, const float* boxes) {
+struct BuildOut {
+	DevLightNode* nodes;
+	int base;
+	Seg* segs;  // every level's segments, level after level (2n - 1 in all)
+	int* total; // segments written so far (shared memory)
+	LightSamples ls;
+};
+
+__device__ __forceinline__ Box node_sample(const LightSamples& ls, int node, int i) {
+	const float* b = ls.nbuf + ((size_t)node * ls.max_ts + i) * 6;
+	Box r;
+	r.lo = V3(b[0], b[1], b[2]);
+	r.hi = V3(b[3], b[4], b[5]);
+	return r;
+}
+
+__device__ __forceinline__ void put_sample(const LightSamples& ls, int node, int i, const Box& x) {
+	float* b = ls.nbuf + ((size_t)node * ls.max_ts + i) * 6;
+	b[0] = x.lo.x; b[1] = x.lo.y; b[2] = x.lo.z;
+	b[3] = x.hi.x; b[4] = x.hi.y; b[5] = x.hi.z;
+}
+
+// A node's bounds in its record: sample 0 in the node, the others in extra
+// records of their own.
+__device__ void store_bounds(const LightSamples& ls, DevLightNode& nd, int node, int ts) {
+	const Box b0 = node_sample(ls, node, 0);
+	nd.lo[0] = b0.lo.x; nd.lo[1] = b0.lo.y; nd.lo[2] = b0.lo.z;
+	nd.hi[0] = b0.hi.x; nd.hi[1] = b0.hi.y; nd.hi[2] = b0.hi.z;
+	nd.ts = ts;
+	int ex = 0;
+	if (ts > 1) {
+		ex = atomicAdd(ls.extra_count, ts - 1);
+		for (int i = 1; i < ts; ++i) {
+			const Box x = node_sample(ls, node, i);
+			float* r = ls.extra + (size_t)(ex + i - 1) * 6;
+			r[0] = x.lo.x; r[1] = x.lo.y; r[2] = x.lo.z;
+			r[3] = x.hi.x; r[4] = x.hi.y; r[5] = x.hi.z;
+		}
+	}
+	nd.extra = ls.extra_base + ex;
+}
+
+__device__ __forceinline__ void write_leaf(const BuildOut& o, const Seg& s, const LightElem* el) {
 	DevLightNode& nd = o.nodes[s.node];
 	const LightElem l = el[s.start];
-	const float* b = boxes + 6 * (size_t)l.box;
-	nd.lo[0] = b[0]; nd.lo[1] = b[1]; nd.lo[2] = b[2];
-	nd.hi[0] = b[3]; nd.hi[1] = b[4]; nd.hi[2] = b[5];
+	const int f = o.ls.first[l.box], ts = o.ls.first[l.box + 1] - f;
+	for (int i = 0; i < ts; ++i) {
+		const float* b = o.ls.samples + 6 * (size_t)(f + i);
+		Box x;
+		x.lo = V3(b[0], b[1], b[2]);
+		x.hi = V3(b[3], b[4], b[5]);
+		put_sample(o.ls, s.node, i, x);
+	}
+	o.ls.nts[s.node] = ts;
+	store_bounds(o.ls, nd, s.node, ts);
 	nd.energy = l.e;
-	nd.ts = 1;
-	nd.extra = o.extra;
 	nd.is_leaf = 1;
 	nd.c1 = l.inst;
 	nd.c2 = 0;
@@ -72,8 +129,6 @@ __device__ __forceinline__ void write_leaf(const BuildOut& o, const Seg& s, cons
 __device__ __forceinline__ void write_inner(const BuildOut& o, const Seg& s, int mid) {
 	DevLightNode& nd = o.nodes[s.node];
 	const int c1 = s.node + 1, c2 = s.node + 2 * (mid - s.start);
-	nd.ts = 1;
-	nd.extra = o.extra;
 	nd.is_leaf = 0;
 	nd.c1 = o.base + c1;
 	nd.c2 = o.base + c2;
@@ -191,8 +246,8 @@ __device__ void warp_split(const BuildOut& o, const Seg& s, LightElem* el, int* 
 
 constexpr int kWarpMin = 33;  // segments of more lights split by a warp
 
-__global__ void __launch_bounds__(kBlock) light_build_kernel(LightElem* __restrict__ el, const float* __restrict__ boxes,
-                                                             int n, int base, int extra, DevLightNode* __restrict__ out,
+__global__ void __launch_bounds__(kBlock) light_build_kernel(LightElem* __restrict__ el, LightSamples ls, int n,
+                                                             int base, DevLightNode* __restrict__ out,
                                                              Seg* __restrict__ segs, int* __restrict__ pos,
                                                              int* __restrict__ level_start) {
 	__shared__ int total, lo, hi, levels;
@@ -205,7 +260,7 @@ __global__ void __launch_bounds__(kBlock) light_build_kernel(LightElem* __restri
 		levels = 0;
 	}
 	__syncthreads();
-	const BuildOut o{out, base, extra, segs, &total};
+	const BuildOut o{out, base, segs, &total, ls};
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	// every level makes every segment of two or more lights strictly smaller,
 	// so there are at most n levels
@@ -220,7 +275,7 @@ __global__ void __launch_bounds__(kBlock) light_build_kernel(LightElem* __restri
 			const Seg s = segs[i];
 			const int size = s.end - s.start;
 			if (size == 1)
-				write_leaf(o, s, el, boxes);
+				write_leaf(o, s, el);
 			else if (size < kWarpMin)
 				thread_split(o, s, el);
 		}
@@ -234,23 +289,37 @@ __global__ void __launch_bounds__(kBlock) light_build_kernel(LightElem* __restri
 		__syncthreads();
 	}
 	// bounds and energies bottom-up, a level's nodes after their children's
-	// (light_tree.cpp:223-229)
+	// (light_tree.cpp:223-229); the bounds merged as the time-sample
+	// sequences of the two children: per sample when they have as many, else
+	// the longer one's samples each with the shorter one interpolated at its
+	// time
 	for (int level = levels - 1; level >= 0; --level) {
 		const int a = level_start[level], b = level_start[level + 1];
 		for (int i = a + (int)threadIdx.x; i < b; i += kBlock) {
-			DevLightNode& nd = out[segs[i].node];
+			const int node = segs[i].node;
+			DevLightNode& nd = out[node];
 			if (nd.is_leaf) continue;
-			const DevLightNode& ca = out[nd.c1 - base];
-			const DevLightNode& cb = out[nd.c2 - base];
-			Box ba, bb;
-			ba.lo = V3(ca.lo[0], ca.lo[1], ca.lo[2]);
-			ba.hi = V3(ca.hi[0], ca.hi[1], ca.hi[2]);
-			bb.lo = V3(cb.lo[0], cb.lo[1], cb.lo[2]);
-			bb.hi = V3(cb.hi[0], cb.hi[1], cb.hi[2]);
-			const Box u = box_union(ba, bb);
-			nd.lo[0] = u.lo.x; nd.lo[1] = u.lo.y; nd.lo[2] = u.lo.z;
-			nd.hi[0] = u.hi.x; nd.hi[1] = u.hi.y; nd.hi[2] = u.hi.z;
-			nd.energy = ca.energy + cb.energy;
+			const int ia = nd.c1 - base, ib = nd.c2 - base;
+			const int ta = ls.nts[ia], tb = ls.nts[ib];
+			const int tl = ta >= tb ? ta : tb;               // the longer sequence
+			const int il = ta >= tb ? ia : ib, is = ta >= tb ? ib : ia;
+			const int tsh = ta >= tb ? tb : ta;
+			for (int k = 0; k < tl; ++k) {
+				Box other;
+				if (ta == tb) {
+					other = node_sample(ls, is, k);
+				} else {
+					const SeqPos sp = seq_pos((float)k / (float)(tl - 1), tsh);
+					other = sp.single ? node_sample(ls, is, sp.i0)
+					                  : box_lerp(sp.nalpha, node_sample(ls, is, sp.i0), node_sample(ls, is, sp.i0 + 1));
+				}
+				// equal lengths: the first child's sample first; else the
+				// longer one's
+				put_sample(ls, node, k, box_union(node_sample(ls, ta == tb ? ia : il, k), other));
+			}
+			ls.nts[node] = tl;
+			store_bounds(ls, nd, node, tl);
+			nd.energy = out[ia].energy + out[ib].energy;
 		}
 		__syncthreads();
 	}
@@ -258,38 +327,56 @@ __global__ void __launch_bounds__(kBlock) light_build_kernel(LightElem* __restri
 
 }  // namespace
 
-cudaError_t build_light_tree_gpu(const float* h_elems, int n, int node_base, int extra, DevLightNode* d_nodes,
-                                 float* root_energy, cudaStream_t st) {
+cudaError_t build_light_tree_gpu(const float* h_elems, const float* h_samples, const int* h_first, int n,
+                                 int node_base, DevLightNode* d_nodes, float* d_extra, int extra_base,
+                                 float* root_energy, int* extra_count, cudaStream_t st) {
+	*extra_count = 0;
 	if (n < 2) return cudaErrorInvalidValue;
 	std::vector<LightElem> el((size_t)n);
-	std::vector<float> boxes(6 * (size_t)n);
+	int max_ts = 1;
 	for (int i = 0; i < n; ++i) {
-		const float* p = h_elems + 11 * (size_t)i;
+		const float* p = h_elems + 5 * (size_t)i;
 		el[i] = LightElem{{p[0], p[1], p[2]}, p[3], (int)p[4], i};
-		for (int k = 0; k < 6; ++k) boxes[6 * (size_t)i + k] = p[5 + k];
+		const int ts = h_first[i + 1] - h_first[i];
+		if (ts < 1) return cudaErrorInvalidValue;
+		max_ts = ts > max_ts ? ts : max_ts;
 	}
+	const size_t n_samples = (size_t)h_first[n];
 	LightElem* d_el = nullptr;
-	float* d_boxes = nullptr;
+	float *d_samples = nullptr, *d_nbuf = nullptr;
 	Seg* d_seg = nullptr;
 	int* d_int = nullptr;
 	cudaError_t e = cudaMalloc(&d_el, sizeof(LightElem) * (size_t)n);
-	if (e == cudaSuccess) e = cudaMalloc(&d_boxes, sizeof(float) * boxes.size());
+	if (e == cudaSuccess) e = cudaMalloc(&d_samples, sizeof(float) * 6 * n_samples);
+	if (e == cudaSuccess) e = cudaMalloc(&d_nbuf, sizeof(float) * 6 * (size_t)max_ts * (2 * (size_t)n - 1));
 	if (e == cudaSuccess) e = cudaMalloc(&d_seg, sizeof(Seg) * (2 * (size_t)n - 1));
-	if (e == cudaSuccess) e = cudaMalloc(&d_int, sizeof(int) * (2 * (size_t)n + 1));
+	// pos (n), level starts (n + 1), first (n + 1), node sample counts
+	// (2n - 1), the extra-record counter (1)
+	if (e == cudaSuccess) e = cudaMalloc(&d_int, sizeof(int) * (5 * (size_t)n + 2));
+	int* d_pos = d_int;
+	int* d_level = d_int + n;
+	int* d_first = d_level + n + 1;
+	int* d_nts = d_first + n + 1;
+	int* d_count = d_nts + 2 * n - 1;
 	if (e == cudaSuccess) e = cudaMemcpyAsync(d_el, el.data(), sizeof(LightElem) * (size_t)n, cudaMemcpyHostToDevice, st);
 	if (e == cudaSuccess)
-		e = cudaMemcpyAsync(d_boxes, boxes.data(), sizeof(float) * boxes.size(), cudaMemcpyHostToDevice, st);
+		e = cudaMemcpyAsync(d_samples, h_samples, sizeof(float) * 6 * n_samples, cudaMemcpyHostToDevice, st);
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(d_first, h_first, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, st);
+	if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, sizeof(int), st);
 	if (e == cudaSuccess) {
-		light_build_kernel<<<1, kBlock, 0, st>>>(d_el, d_boxes, n, node_base, extra, d_nodes, d_seg, d_int,
-		                                         d_int + n);
+		const LightSamples ls{d_samples, d_first, d_nbuf, d_nts, max_ts, d_extra, d_count, extra_base};
+		light_build_kernel<<<1, kBlock, 0, st>>>(d_el, ls, n, node_base, d_nodes, d_seg, d_pos, d_level);
 		e = cudaGetLastError();
 	}
 	if (e == cudaSuccess)
 		e = cudaMemcpyAsync(root_energy, &d_nodes[0].energy, sizeof(float), cudaMemcpyDeviceToHost, st);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(extra_count, d_count, sizeof(int), cudaMemcpyDeviceToHost, st);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(st);
 	cudaFree(d_int);
 	cudaFree(d_seg);
-	cudaFree(d_boxes);
+	cudaFree(d_nbuf);
+	cudaFree(d_samples);
 	cudaFree(d_el);
 	return e;
 }

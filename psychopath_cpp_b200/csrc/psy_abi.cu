@@ -619,7 +619,7 @@ int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags
 	ctx->gpu_light_nodes = -1;
 	if (b->gpu_light_pending) {
 		// the host-built light nodes, then the root's device-built tree
-		const int n = (int)(b->gpu_light_elems.size() / 11);
+		const int n = (int)b->gpu_light_first.size() - 1;
 		const size_t host_nodes = b->light_nodes.size();
 		const size_t cap = host_nodes + 2 * (size_t)n - 1;
 		void* lp = nullptr;
@@ -629,25 +629,44 @@ int psy_scene_upload_ex(psy_ctx* ctx, const psy_scene_desc* desc, uint32_t flags
 		if (host_nodes && (rc = ctx_cuda(ctx, cudaMemcpy(lp, b->light_nodes.data(), host_nodes * sizeof(DevLightNode),
 		                                                 cudaMemcpyHostToDevice), "cudaMemcpy(light_nodes)")))
 			return rc;
+		// the host-built nodes' later bounds samples, then room for the device
+		// nodes' (at most one record per sample after the first)
+		int most = 1;
+		for (int i = 0; i < n; ++i) most = std::max(most, b->gpu_light_first[i + 1] - b->gpu_light_first[i]);
+		const size_t host_extra = b->light_extra.size();
+		const size_t extra_cap = host_extra + (2 * (size_t)n - 1) * (size_t)(most - 1) * 6;
+		void* xp = nullptr;
+		if ((rc = ctx_cuda(ctx, cudaMalloc(&xp, (extra_cap ? extra_cap : 1) * sizeof(float)),
+		                   "cudaMalloc(light_extra)")))
+			return rc;
+		ctx->scene_allocs.push_back(xp);
+		ctx->device_bytes += extra_cap * sizeof(float);
+		if (host_extra && (rc = ctx_cuda(ctx, cudaMemcpy(xp, b->light_extra.data(), host_extra * sizeof(float),
+		                                                 cudaMemcpyHostToDevice), "cudaMemcpy(light_extra)")))
+			return rc;
 		float energy = 0.0f;
-		if ((rc = ctx_cuda(ctx, build_light_tree_gpu(b->gpu_light_elems.data(), n, (int)host_nodes,
-		                                             (int)(b->light_extra.size() / 6),
-		                                             static_cast<DevLightNode*>(lp) + host_nodes, &energy, nullptr),
+		int extras = 0;
+		if ((rc = ctx_cuda(ctx, build_light_tree_gpu(b->gpu_light_elems.data(), b->gpu_light_samples.data(),
+		                                             b->gpu_light_first.data(), n, (int)host_nodes,
+		                                             static_cast<DevLightNode*>(lp) + host_nodes,
+		                                             static_cast<float*>(xp) + host_extra, (int)(host_extra / 6),
+		                                             &energy, &extras, nullptr),
 		                   "psy_scene_upload_ex: device light tree build")))
 			return rc;
+		d.light_extra = static_cast<const float*>(xp);
 		b->assemblies[0].light_root = (int)host_nodes;
 		b->assemblies[0].light_energy = energy;
 		ctx->gpu_light_nodes = 2 * n - 1;
 		d.light_nodes = static_cast<const DevLightNode*>(lp);
 	} else {
 		UP(light_nodes, b->light_nodes);
+		UP(light_extra, b->light_extra);
 	}
 	UP(assemblies, b->assemblies);
 	UP(instances, b->instances);
 	UP(objects, b->objects);
 	UP(xforms, b->xforms);
 	UP(fpool, b->fpool);
-	UP(light_extra, b->light_extra);
 	UP(shaders, b->shaders);
 	UP(cam_xforms, b->cam_xforms);
 	UP(cam_tfovs, b->cam_tfovs);

@@ -830,15 +830,15 @@ struct Builder {
 	}
 
 	// The lights of the root for the device build of its light tree, when
-	// it has two or more and each light's bounds have one time sample
-	// (every node then has one box); false otherwise.
+	// it has two or more and each light has bounds; false otherwise.
 	bool light_tree_for_gpu(HAssembly& ha, int aidx) {
 		std::vector<LBuild> bn;
 		uint32_t total_lights = 0;
 		collect_lights(ha, bn, total_lights);
 		if (bn.size() < 2) return false;
-		std::vector<float> el;
-		el.reserve(bn.size() * 11);
+		std::vector<float> el, samples;
+		std::vector<int> first{0};
+		el.reserve(bn.size() * 5);
 		for (const LBuild& l : bn) {
 			const psy_instance_desc& id = ha.d->instances[l.instance];
 			std::vector<Box> bb;
@@ -850,11 +850,14 @@ struct Builder {
 				                                             (int)id.transform_count)
 				                            : sub.light_bounds;
 			}
-			if (bb.size() != 1 || l.instance >= (1u << 24)) return false;
-			el.insert(el.end(), {l.center.x, l.center.y, l.center.z, l.energy, (float)l.instance, bb[0].lo.x,
-			                     bb[0].lo.y, bb[0].lo.z, bb[0].hi.x, bb[0].hi.y, bb[0].hi.z});
+			if (bb.empty() || bb.size() > 64 || l.instance >= (1u << 24)) return false;
+			el.insert(el.end(), {l.center.x, l.center.y, l.center.z, l.energy, (float)l.instance});
+			for (const Box& b : bb) samples.insert(samples.end(), {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z});
+			first.push_back(first.back() + (int)bb.size());
 		}
 		out->gpu_light_elems.swap(el);
+		out->gpu_light_samples.swap(samples);
+		out->gpu_light_first.swap(first);
 		out->gpu_light_pending = true;
 		DevAssembly& da = out->assemblies[aidx];
 		da.light_root = -1;  // set by the device build

@@ -49,19 +49,21 @@ struct BuiltScene {
 	std::vector<float> gpu_leaf_boxes;    // every root instance's time samples: lo xyz, hi xyz
 	std::vector<int> gpu_leaf_first;      // instance i's samples: [first[i], first[i + 1])
 	std::vector<float> gpu_leaf_centres;  // per root instance: its box's centre at time 0.5
-	// With gpu_root_bvh requested and a root with two or more lights whose
-	// bounds have one time sample each, the root's light tree is left to the
-	// device build: its lights in LightTree::build's order, 11 floats each
-	// (centre xyz, energy, local instance index, bounds lo xyz, hi xyz), and
-	// assemblies[0].light_root stays -1 until that build sets it.
+	// With gpu_root_bvh requested and a root with two or more lights, the
+	// root's light tree is left to the device build: its lights in
+	// LightTree::build's order, 5 floats each (centre xyz, energy, local
+	// instance index), their bounds' time samples (6 floats each, light i's
+	// are [first[i], first[i + 1])), and assemblies[0].light_root stays -1
+	// until that build sets it.
 	bool gpu_light_pending = false;
 	std::vector<float> gpu_light_elems;
+	std::vector<float> gpu_light_samples;
+	std::vector<int> gpu_light_first;
 };
 
 // Validates the description and builds every assembly (children first).
-// gpu_root_bvh: leave the root assembly's traversal tree and (when its
-// lights do not move) its light tree to the device builds (see
-// gpu_root_pending and gpu_light_pending).  Returns PSY_OK or
+// gpu_root_bvh: leave the root assembly's traversal tree and light tree to
+// the device builds (see gpu_root_pending and gpu_light_pending).  Returns PSY_OK or
 // PSY_ERR_ARG with *err set.
 int build_scene(const psy_scene_desc* desc, BuiltScene* out, std::string* err, bool gpu_root_bvh = false);
 

@@ -70,7 +70,35 @@ def _stacked_light_scene(n_lights, seed):
     return sc
 
 
-@pytest.mark.parametrize("which", ["plain", "many", "bench", "stacked"])
+def _moving_light_scene(n_lights, seed):
+    """Sphere lights with one to three time samples of position and radius
+    (moving bounds, sample counts mixed so that merged bounds interpolate),
+    and an assembly of lights instanced with one- and two-sample
+    transforms."""
+    from psychopath_cpp_b200.scene import Assembly, SphereLight
+    sc = scenes.plain_scene(4)
+    rng = np.random.default_rng(seed)
+    for k in range(n_lights):
+        ts = int(rng.integers(1, 4))
+        p0 = rng.uniform((-5, -5, 2), (5, 5, 6))
+        locs = [p0 + rng.normal(0, 0.4, 3) * j for j in range(ts)]
+        sc.root.add_object("ml%d" % k, SphereLight(locs, rng.uniform(0.05, 0.3, ts),
+                                                   [[float(rng.uniform(1, 40))] * 3] * ts))
+        sc.root.add_instance("ml%d" % k)
+    lamp = Assembly()
+    lamp.add_object("bulb", SphereLight([[0.0, 0.0, 0.0]], [0.2], [[30.0] * 3]))
+    lamp.add_instance("bulb")
+    sc.root.add_assembly("lamp", lamp)
+    for k in range(12):
+        ax = rng.normal(size=3)
+        t0 = rng.uniform((-4, -4, 2), (4, 4, 5))
+        m0 = scenes.placement(ax, 0.3, t0)
+        xf = [m0] if k % 3 == 0 else [m0, scenes.placement(ax, 0.4, t0 + rng.normal(0, 0.3, 3))]
+        sc.root.add_instance("lamp", xf)
+    return sc
+
+
+@pytest.mark.parametrize("which", ["plain", "many", "bench", "stacked", "moving"])
 def test_light_tree_sample_parity(ctx, ref_available, which):
     """LightTree::sample; "bench" is the 720p benchmark scene's own tree
     (10,000 sphere lights, 19,999 nodes) with queries over its ground;
@@ -79,6 +107,9 @@ def test_light_tree_sample_parity(ctx, ref_available, which):
     if which == "stacked":
         sc = _stacked_light_scene(400, 9)
         q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 6), 4)
+    elif which == "moving":
+        sc = _moving_light_scene(300, 10)
+        q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 6), 6)
     elif which == "plain":
         sc = scenes.plain_scene(4)
         q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 3), 1)
@@ -100,7 +131,7 @@ def test_light_tree_sample_parity(ctx, ref_available, which):
         assert d.max() == 0, (name, int((d > 0).sum()), int(d.max()))
 
 
-@pytest.mark.parametrize("which", ["plain", "rect", "many", "bench", "stacked"])
+@pytest.mark.parametrize("which", ["plain", "rect", "many", "bench", "stacked", "moving"])
 def test_device_light_tree_matches_host(ctx, which):
     """The root's light tree built on the device (upload with gpu_bvh) is
     LightTree::build's tree node for node: every light choice and output bit
@@ -109,6 +140,9 @@ def test_device_light_tree_matches_host(ctx, which):
     if which == "stacked":
         sc = _stacked_light_scene(400, 9)
         q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 6), 4)
+    elif which == "moving":
+        sc = _moving_light_scene(300, 10)
+        q = _light_queries(40000, (-6, -6, 0.0), (6, 6, 6), 6)
     elif which == "plain":
         sc = scenes.plain_scene(4)
         q = _light_queries(20000, (-6, -6, 0.0), (6, 6, 3), 1)
@@ -129,7 +163,7 @@ def test_device_light_tree_matches_host(ctx, which):
     dev = ctx.stats()
     assert dev["light_nodes"] == host["light_nodes"]
     # the root's lights (one sphere in the plain scene: nothing to build)
-    n_root = {"plain": 0, "rect": 2, "many": 2000, "bench": 10000, "stacked": 401}[which]
+    n_root = {"plain": 0, "rect": 2, "many": 2000, "bench": 10000, "stacked": 401, "moving": 313}[which]
     assert dev["gpu_light_nodes"] == (2 * n_root - 1 if n_root > 1 else 0)
     b, idb = api.LightTree(ctx).sample(q)
     assert (ida == idb).all(), int((ida != idb).sum())
