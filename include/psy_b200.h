@@ -146,7 +146,7 @@ int psy_scene_upload(psy_ctx* ctx, const psy_scene_desc* scene);
  * included), so traces and renders are those of psy_scene_upload bit for
  * bit.  The root's
  * light tree is built on the device too, when it has two or more lights
- * whose bounds have no motion: LightTree::build's own tree node for node
+ * (moving bounds included): LightTree::build's own tree node for node
  * (accel/light_tree.cpp:99-238, libstdc++'s partition order included), so
  * light selection is unchanged.  The nested assemblies' trees are built on
  * the host either way.
