@@ -190,6 +190,50 @@ def test_nan_differentials_end_at_min_upoly(ctx, ref_available):
         np.testing.assert_array_equal(mine_zero[k], mine_nan[k])
 
 
+def _edge_scene(kind):
+    """Small root shapes for the device builds: two instances, one
+    instance, and 40 instances on one centre (no bin boundary separates
+    them, so every split among them is the midpoint split peeling one off;
+    the tree is as deep as the traversal's 64-entry node stack allows, the
+    size of the reference's, accel/bvh4.hpp:161)."""
+    from psychopath_cpp_b200.scene import Scene, Sphere, SphereLight
+    sc = Scene(name="edge_" + kind, res_x=32, res_y=24, spp=1, seed=1)
+    sc.camera = scenes.Camera(transforms=[scenes.look_at((0.0, -8.0, 3.0), (0.0, 0.0, 0.5))], fovs=[45.0])
+    root = sc.root
+    root.add_shader("m", scenes.SurfaceShader("Lambert", [0.7, 0.7, 0.7]))
+    if kind == "two":
+        root.add_object("s0", Sphere([-1.0, 0.0, 0.5], 0.8))
+        root.add_instance("s0", shader="m")
+    elif kind == "stacked":
+        rng = np.random.default_rng(3)
+        for k in range(40):
+            root.add_object("s%d" % k, Sphere([0.0, 0.0, 0.5], float(rng.uniform(0.2, 1.5))))
+            root.add_instance("s%d" % k, shader="m")
+    # one light in every scene ("one": the light is the only instance)
+    root.add_object("light", SphereLight([[1.0, -1.0, 4.0]], [0.4], [[50.0] * 3]))
+    root.add_instance("light")
+    return sc
+
+
+@pytest.mark.parametrize("kind", ["two", "one", "stacked"])
+def test_device_built_bvh_edge_cases(ctx, kind):
+    """The device BVH4 build on the smallest and most degenerate roots:
+    every trace output bit equal to the host-built tree's."""
+    sc = _edge_scene(kind)
+    rays = parity.random_rays(20000, (-3, -3, -0.5), (3, 3, 5), seed=47, occl_frac=0.3, width=0.002)
+    fields = ("hit", "id", "t", "uv", "closure")
+    ctx.upload(sc)
+    host_st = ctx.stats()
+    a = api.Tracer(ctx).trace(rays, fields=fields)
+    ctx.upload(sc, gpu_bvh=True)
+    st = ctx.stats()
+    b = api.Tracer(ctx).trace(rays, fields=fields)
+    assert st["bvh4_nodes"] == host_st["bvh4_nodes"]
+    assert a["hit"].sum() > 0
+    for k in fields:
+        np.testing.assert_array_equal(np.asarray(a[k]).view(np.uint8), np.asarray(b[k]).view(np.uint8))
+
+
 @pytest.mark.parametrize("kind", ["batch", "heightfield", "motion", "motion_patch"])
 def test_device_built_bvh_gives_the_same_hits(ctx, ref_available, kind):
     """psy_scene_upload_ex(PSY_UPLOAD_GPU_BVH): the root's traversal BVH4
