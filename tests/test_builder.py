@@ -139,3 +139,51 @@ def test_malformed_descriptions_are_rejected():
     desc.cam_transform_count = 0
     assert L.psy_build_bvh4(C.byref(desc), 0, C.byref(n), None, None, None, None) == _abi.PSY_ERR_ARG
     del keep
+
+
+def _two_ended_partition(v, pred):
+    """std::partition on random-access iterators as libstdc++ writes it (the
+    order the reference's BVH and light-tree splits leave their elements in)."""
+    v = list(v)
+    first, last = 0, len(v)
+    while True:
+        while first != last and pred(v[first]):
+            first += 1
+        if first == last:
+            return v, first
+        last -= 1
+        while first != last and not pred(v[last]):
+            last -= 1
+        if first == last:
+            return v, first
+        v[first], v[last] = v[last], v[first]
+        first += 1
+
+
+def _closed_form_partition(v, pred):
+    """The device builds' warp partition: with m elements satisfying the
+    predicate, exchange the k-th one failing it among the first m positions
+    (from the front) with the k-th one satisfying it among the others (from
+    the back)."""
+    v = list(v)
+    m = sum(1 for x in v if pred(x))
+    front = [i for i in range(m) if not pred(v[i])]
+    back = [j for j in range(len(v) - 1, m - 1, -1) if pred(v[j])]
+    assert len(front) == len(back)
+    for i, j in zip(front, back):
+        v[i], v[j] = v[j], v[i]
+    return v, m
+
+
+def test_closed_form_partition_is_the_two_ended_loop():
+    """The element order (and partition point) of the device builds' warp
+    partition equals libstdc++'s two-ended loop, on ragged and empty inputs,
+    all-true and all-false predicates and heavy duplicates."""
+    rng = np.random.default_rng(5)
+    cases = [([], 1), ([(3, 0)], 1), ([(3, 0)], 5)]
+    for trial in range(3000):
+        n = int(rng.integers(1, 100))
+        cases.append(([(int(rng.integers(0, 8)), k) for k in range(n)], int(rng.integers(0, 9))))
+    for v, th in cases:
+        pred = lambda x, th=th: x[0] < th
+        assert _two_ended_partition(v, pred) == _closed_form_partition(v, pred), (v, th)
