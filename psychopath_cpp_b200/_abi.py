@@ -86,6 +86,10 @@ class SceneStats(C.Structure):
                 ("device_bytes", C.c_uint64), ("gpu_bvh4_nodes", C.c_uint32), ("gpu_light_nodes", C.c_uint32)]
 
 
+class RenderSettings(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("seed", C.c_uint32)]
+
+
 class RaySoA(C.Structure):
     _fields_ = [("o", C.c_void_p), ("d", C.c_void_p), ("odx", C.c_void_p), ("ody", C.c_void_p),
                 ("ddx", C.c_void_p), ("ddy", C.c_void_p), ("time", C.c_void_p), ("type", C.c_void_p)]
@@ -146,7 +150,8 @@ EXPORTED = ["psy_ctx_create", "psy_ctx_destroy", "psy_last_error", "psy_version"
             "psy_scene_stats_get", "psy_build_bvh4", "psy_build_light_tree", "psy_trace", "psy_trace_host", "psy_sync",
             "psy_trace_host_noalloc", "psy_render_batch", "psy_batch_autotune", "psy_render_diff",
             "psy_render_adjoint", "psy_profile_enable", "psy_profile_read", "psy_profile_counters",
-            "psy_light_sample", "psy_render", "psy_film_srgb8", "psy_math_check"]
+            "psy_light_sample", "psy_render", "psy_film_srgb8", "psy_math_check", "psy_file_parse",
+            "psy_file_scene_desc", "psy_file_render_settings", "psy_file_free"]
 
 _lib = None
 
@@ -200,6 +205,13 @@ def load():
     if hasattr(L, "psy_render"):
         L.psy_render.argtypes = [C.c_void_p, C.POINTER(RenderDesc), C.c_void_p, C.c_void_p,
                                  C.POINTER(RenderStats), C.c_void_p]
+    if hasattr(L, "psy_file_parse"):
+        L.psy_file_parse.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]
+        L.psy_file_scene_desc.argtypes = [C.c_void_p]
+        L.psy_file_scene_desc.restype = C.POINTER(SceneDesc)
+        L.psy_file_render_settings.argtypes = [C.c_void_p, C.POINTER(RenderSettings)]
+        L.psy_file_free.argtypes = [C.c_void_p]
+        L.psy_file_free.restype = None
     _lib = L
     return L
 

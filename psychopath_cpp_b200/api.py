@@ -143,6 +143,50 @@ def flatten(scene: Scene):
     return d, keep
 
 
+class PsyFile:
+    """A .psy scene file read by the library (psy_file_parse), in place of
+    the reference's Parser::parse_scene (parser/parser.cpp:37-662): its
+    scene description and render settings.  Context.upload_flat(f.flat())
+    uploads it; build_bvh4_records / build_light_tree take it too."""
+
+    def __init__(self, text: str):
+        self.L = _abi.load()
+        data = text.encode() if isinstance(text, str) else bytes(text)
+        h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        rc = self.L.psy_file_parse(data, len(data), C.byref(h), err, len(err))
+        if rc != 0:
+            raise _abi.PsyError(rc, err.value.decode())
+        self.h = h
+        s = _abi.RenderSettings()
+        self.L.psy_file_render_settings(h, C.byref(s))
+        self.settings = {k: int(getattr(s, k)) for k, _ in _abi.RenderSettings._fields_}
+
+    @classmethod
+    def read(cls, path: str) -> "PsyFile":
+        with open(path) as f:
+            return cls(f.read())
+
+    @property
+    def desc(self):
+        return self.L.psy_file_scene_desc(self.h).contents
+
+    def flat(self):
+        """(SceneDesc, keepalive), the form flatten() returns."""
+        return self.desc, self
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.psy_file_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # --------------------------------------------------------------------------
 # Context and reference-named wrappers
 # --------------------------------------------------------------------------
@@ -233,7 +277,7 @@ def build_bvh4_records(scene: Scene, assembly: int = 0) -> dict:
     """Host-only: the BVH4 node records the builder produces for one
     assembly, in the reference's BVH4::Node form (psy_build_bvh4)."""
     L = _abi.load()
-    desc, keep = flatten(scene)
+    desc, keep = scene.flat() if isinstance(scene, PsyFile) else flatten(scene)
     n = C.c_uint64()
     _check(L, L.psy_build_bvh4(C.byref(desc), assembly, C.byref(n), None, None, None, None), "psy_build_bvh4")
     k = n.value
@@ -252,7 +296,7 @@ def build_light_tree(scene: Scene, assembly: int = 0) -> dict:
     """Host-only: the light tree the builder produces for one assembly
     (psy_build_light_tree), in the reference's LightTree node form."""
     L = _abi.load()
-    desc, keep = flatten(scene)
+    desc, keep = scene.flat() if isinstance(scene, PsyFile) else flatten(scene)
     n, nb, lc = C.c_uint64(), C.c_uint64(), C.c_uint64()
     te = C.c_float()
     _check(L, L.psy_build_light_tree(C.byref(desc), assembly, C.byref(n), C.byref(nb), None, None, None,

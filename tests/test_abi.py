@@ -60,7 +60,7 @@ _MIRRORS = {
     "RaySoA": "psy_ray_soa", "HitSoA": "psy_hit_soa", "LightQuerySoA": "psy_light_query_soa",
     "LightSampleSoA": "psy_light_sample_soa", "RenderDesc": "psy_render_desc", "DiffDesc": "psy_diff_desc",
     "BatchDesc": "psy_batch_desc", "BatchTuning": "psy_batch_tuning", "RenderStats": "psy_render_stats",
-    "TraceCounters": "psy_trace_counters",
+    "TraceCounters": "psy_trace_counters", "RenderSettings": "psy_render_settings",
 }
 
 

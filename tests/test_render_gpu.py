@@ -179,6 +179,20 @@ def test_device_light_tree_matches_host(ctx, which):
         assert (np.asarray(x).view(np.uint32) == np.asarray(y).view(np.uint32)).all()
 
 
+def test_psy_file_upload_renders_the_same(ctx):
+    """A scene read from its .psy file by the library (psy_file_parse)
+    uploads and renders bit for bit as the same scene built in Python."""
+    sc = scenes.many_light_scene(7, res=(48, 27), spp=4, n_patches=80, n_groups=40, n_lights=500)
+    ctx.upload(sc)
+    a, ca = api.PathTraceIntegrator(ctx, 48, 27, 4, seed=1, path_length=4).integrate()
+    f = api.PsyFile(sc.to_psy())
+    assert f.settings == {"width": 48, "height": 27, "spp": 4, "seed": sc.seed}
+    ctx.upload_flat(f.flat())
+    b, cb = api.PathTraceIntegrator(ctx, 48, 27, 4, seed=1, path_length=4).integrate()
+    assert (np.asarray(a).view(np.uint32) == np.asarray(b).view(np.uint32)).all()
+    assert (np.asarray(ca) == np.asarray(cb)).all()
+
+
 def test_plain_render_matches_reference(ctx, ref_available):
     sc = scenes.plain_scene(1, res=(80, 60), spp=16)
     (rx, rc, rrays), (mx, mc, mrays) = _render_both(ctx, sc, 16, 4)
