@@ -188,21 +188,22 @@ int psy_build_light_tree(const psy_scene_desc* scene, uint32_t assembly, uint64_
 
 /*
  * Host-only: a .psy scene file read into a scene description, replacing the
- * reference's Parser::parse_scene (parser/data_tree.cpp:177-400,
- * parser/parser.cpp:37-662): the first Scene node's render settings,
+ * reference's Parser::parse_next_frame (parser/data_tree.cpp:177-400,
+ * parser/parser.cpp:37-662): the frame-th Scene node's render settings,
  * camera, background colour and root assembly (shaders, spheres, bilinear
  * and bicubic patches, sphere and rectangle lights, nested assemblies,
  * instances with motion transforms and shader bindings).  Numbers are read
  * as the reference reads them (std::stof of each -?[0-9]+[.]?[0-9]* match).
  * psy_file_parse returns PSY_ERR_ARG for a malformed file, with the reason
- * in err (err_len bytes, NULL for none); the description stays valid until
- * psy_file_free.
+ * in err (err_len bytes, NULL for none), and PSY_ERR_NO_SCENE when the file
+ * has no Scene node `frame` (frames count from 0: where parse_next_frame
+ * returns null); the description stays valid until psy_file_free.
  */
 typedef struct psy_file_scene psy_file_scene;
 typedef struct psy_render_settings {
 	uint32_t width, height, spp, seed;  /* RenderSettings: Resolution, SamplesPerPixel, Seed */
 } psy_render_settings;
-int psy_file_parse(const char* text, size_t len, psy_file_scene** out, char* err, size_t err_len);
+int psy_file_parse(const char* text, size_t len, uint32_t frame, psy_file_scene** out, char* err, size_t err_len);
 const psy_scene_desc* psy_file_scene_desc(const psy_file_scene* scene);
 int psy_file_render_settings(const psy_file_scene* scene, psy_render_settings* out);
 void psy_file_free(psy_file_scene* scene);

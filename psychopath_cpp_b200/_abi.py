@@ -206,7 +206,8 @@ def load():
         L.psy_render.argtypes = [C.c_void_p, C.POINTER(RenderDesc), C.c_void_p, C.c_void_p,
                                  C.POINTER(RenderStats), C.c_void_p]
     if hasattr(L, "psy_file_parse"):
-        L.psy_file_parse.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]
+        L.psy_file_parse.argtypes = [C.c_char_p, C.c_size_t, C.c_uint32, C.POINTER(C.c_void_p), C.c_char_p,
+                                     C.c_size_t]
         L.psy_file_scene_desc.argtypes = [C.c_void_p]
         L.psy_file_scene_desc.restype = C.POINTER(SceneDesc)
         L.psy_file_render_settings.argtypes = [C.c_void_p, C.POINTER(RenderSettings)]

@@ -147,14 +147,16 @@ class PsyFile:
     """A .psy scene file read by the library (psy_file_parse), in place of
     the reference's Parser::parse_scene (parser/parser.cpp:37-662): its
     scene description and render settings.  Context.upload_flat(f.flat())
-    uploads it; build_bvh4_records / build_light_tree take it too."""
+    uploads it; build_bvh4_records / build_light_tree take it too.  `frame`
+    picks the file's Scene node (parse_next_frame reads them in order; past
+    the last one raises PsyError with code PSY_ERR_NO_SCENE)."""
 
-    def __init__(self, text: str):
+    def __init__(self, text: str, frame: int = 0):
         self.L = _abi.load()
         data = text.encode() if isinstance(text, str) else bytes(text)
         h = C.c_void_p()
         err = C.create_string_buffer(512)
-        rc = self.L.psy_file_parse(data, len(data), C.byref(h), err, len(err))
+        rc = self.L.psy_file_parse(data, len(data), frame, C.byref(h), err, len(err))
         if rc != 0:
             raise _abi.PsyError(rc, err.value.decode())
         self.h = h
@@ -163,9 +165,9 @@ class PsyFile:
         self.settings = {k: int(getattr(s, k)) for k, _ in _abi.RenderSettings._fields_}
 
     @classmethod
-    def read(cls, path: str) -> "PsyFile":
+    def read(cls, path: str, frame: int = 0) -> "PsyFile":
         with open(path) as f:
-            return cls(f.read())
+            return cls(f.read(), frame)
 
     @property
     def desc(self):

@@ -391,15 +391,20 @@ struct SceneRead {
 	psy_render_settings settings{64, 64, 1, 1};
 };
 
-// The first Scene node (parser/parser.cpp:37-184).
-SceneRead read_scene(const Node& tree) {
+struct NoFrame {};
+
+// The frame-th Scene node (parser/parser.cpp:37-184; parse_next_frame reads
+// them in file order).
+SceneRead read_scene(const Node& tree, uint32_t frame) {
 	const Node* sn = nullptr;
+	uint32_t k = 0;
 	for (const Node& c : tree.children)
-		if (c.type == "Scene") {
+		if (c.type == "Scene" && k++ == frame) {
 			sn = &c;
 			break;
 		}
-	if (!sn) throw ParseError{"no Scene node"};
+	if (!sn && frame == 0) throw ParseError{"no Scene node"};
+	if (!sn) throw NoFrame{};
 	SceneRead s;
 	for (const Node& node : sn->children) {
 		if (node.type == "RenderSettings") {
@@ -550,16 +555,20 @@ void flatten(SceneRead& s, psy_file_scene* f) {
 
 }  // namespace
 
-extern "C" int psy_file_parse(const char* text, size_t len, psy_file_scene** out, char* err, size_t err_len) {
+extern "C" int psy_file_parse(const char* text, size_t len, uint32_t frame, psy_file_scene** out, char* err,
+                              size_t err_len) {
 	if (!out || (len && !text)) return PSY_ERR_ARG;
 	*out = nullptr;
 	try {
 		const Node tree = build_tree(tokenize(text, len));
-		SceneRead s = read_scene(tree);
+		SceneRead s = read_scene(tree, frame);
 		std::unique_ptr<psy_file_scene> f(new psy_file_scene());
 		flatten(s, f.get());
 		*out = f.release();
 		return PSY_OK;
+	} catch (const NoFrame&) {
+		if (err && err_len) std::snprintf(err, err_len, "no Scene node %u", frame);
+		return PSY_ERR_NO_SCENE;
 	} catch (const ParseError& e) {
 		if (err && err_len) std::snprintf(err, err_len, "%s", e.msg.c_str());
 	} catch (const std::exception& e) {

@@ -239,3 +239,20 @@ def test_library_reader_reads_back_the_written_scene(make):
     sc = make()
     d, keep = api.flatten(sc)
     assert _desc_dict(api.PsyFile(sc.to_psy()).desc) == _desc_dict(d)
+
+
+def test_library_reader_frames():
+    """A file of several Scene nodes read frame by frame, as the reference's
+    parse_next_frame reads them; past the last frame, PSY_ERR_NO_SCENE."""
+    from psychopath_cpp_b200 import _abi, api
+    a = scenes.plain_scene(1, res=(8, 6), spp=1, n_spheres=3)
+    b = scenes.rect_light_scene(1, res=(10, 4), spp=3, n_spheres=2)
+    txt = a.to_psy() + "\n" + b.to_psy()
+    for frame, sc in enumerate((a, b)):
+        f = api.PsyFile(txt, frame)
+        d, keep = api.flatten(sc)
+        assert _desc_dict(f.desc) == _desc_dict(d)
+        assert f.settings["width"] == sc.res_x and f.settings["spp"] == sc.spp
+    with pytest.raises(_abi.PsyError) as e:
+        api.PsyFile(txt, 2)
+    assert e.value.code == _abi.PSY_ERR_NO_SCENE
