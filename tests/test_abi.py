@@ -87,3 +87,61 @@ def test_ctypes_mirrors_match_the_header_layout(tmp_path):
     subprocess.run(["gcc", "-std=c99", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     assert got == expect
+
+
+C_CONSUMER = r"""
+#include <stdio.h>
+#include <stdlib.h>
+#include "psy_b200.h"
+int main(int argc, char** argv) {
+    FILE* fp = fopen(argv[1], "rb");
+    if (!fp) return 2;
+    fseek(fp, 0, SEEK_END);
+    long n = ftell(fp);
+    fseek(fp, 0, SEEK_SET);
+    char* text = (char*)malloc((size_t)n);
+    if (fread(text, 1, (size_t)n, fp) != (size_t)n) return 3;
+    fclose(fp);
+    psy_file_scene* f = NULL;
+    char err[256];
+    if (psy_file_parse(text, (size_t)n, 0, &f, err, sizeof err) != PSY_OK) { printf("error %s\n", err); return 4; }
+    const psy_scene_desc* d = psy_file_scene_desc(f);
+    psy_render_settings rs;
+    psy_file_render_settings(f, &rs);
+    uint64_t nodes = 0;
+    if (psy_build_bvh4(d, 0, &nodes, NULL, NULL, NULL, NULL) != PSY_OK) return 5;
+    printf("%u %u %u %u %u %u %llu\n", rs.width, rs.height, rs.spp, d->assembly_count,
+           d->assemblies[0].instance_count, d->shader_count, (unsigned long long)nodes);
+    psy_file_free(f);
+    free(text);
+    return 0;
+}
+"""
+
+
+def test_c_program_reads_a_scene_file(tmp_path):
+    """The C ABI from plain C (no Python in between): a program compiled by
+    gcc against include/psy_b200.h and linked to the library reads a .psy
+    file and builds its root BVH4 on the host, with the Python path's
+    counts."""
+    import shutil
+    import subprocess
+    from psychopath_cpp_b200 import api, scenes
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    L = _abi.load()
+    lib = L._name
+    sc = scenes.many_light_scene(2, res=(32, 18), spp=2, n_patches=12, n_groups=10, n_lights=20)
+    path = tmp_path / "s.psy"
+    sc.write_psy(str(path))
+    src = tmp_path / "consumer.c"
+    src.write_text(C_CONSUMER)
+    exe = tmp_path / "consumer"
+    libdir = os.path.dirname(lib)
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe), lib,
+                    "-Wl,-rpath," + libdir], check=True)
+    out = subprocess.run([str(exe), str(path)], check=True, capture_output=True, text=True).stdout.split()
+    d, keep = api.flatten(sc)
+    nodes = api.build_bvh4_records(sc, 0)["ts"].shape[0]
+    assert [int(x) for x in out] == [sc.res_x, sc.res_y, sc.spp, d.assembly_count, d.assemblies[0].instance_count,
+                                     d.shader_count, nodes]
