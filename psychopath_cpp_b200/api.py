@@ -171,7 +171,11 @@ class PsyFile:
 
     @property
     def desc(self):
-        return self.L.psy_file_scene_desc(self.h).contents
+        """The scene description; it keeps this reader (and the memory it
+        points into) alive."""
+        d = self.L.psy_file_scene_desc(self.h).contents
+        d._owner = self
+        return d
 
     def flat(self):
         """(SceneDesc, keepalive), the form flatten() returns."""

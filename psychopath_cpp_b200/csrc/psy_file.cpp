@@ -10,11 +10,18 @@
  *   - numbers are read from a leaf's contents as the reference reads them:
  *     every match of -?[0-9]+[.]?[0-9]* (integers: -?[0-9]+), converted by
  *     std::stof / std::stoi;
- *   - the flattening is the one the Python scene model's flatten() does:
- *     assemblies depth first in declaration order (the root first), objects
- *     and sub-assemblies in declaration order, shaders numbered in the order
- *     instances first bind them (looked up through the enclosing
- *     assemblies, scene/assembly.hpp:113-121).
+ *   - names as the reference's Assembly keeps them (scene/assembly.hpp:
+ *     104-157): every definition is kept in order, and a name finds its
+ *     first definition; names match as written, $ included;
+ *   - an instance's shader is bound when the instance is read, to the
+ *     shader of that name defined so far in its assembly or else in the
+ *     enclosing ones (parser/parser.cpp:298-323, assembly.hpp:113-121);
+ *   - where the reference prints an error and goes on (an instance of
+ *     unknown data is dropped, an unknown shader binds none), the file is
+ *     rejected instead;
+ *   - the flattening: assemblies depth first in declaration order (the root
+ *     first), objects and sub-assemblies in declaration order, shaders
+ *     numbered in the order instances first bind them.
  */
 #include <cctype>
 #include <cstdio>
@@ -188,7 +195,6 @@ void fill(const std::string& s, float* out, size_t count, const float* def) {
 const float kIdentity[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
 const float kZero3[3] = {0, 0, 0};
 
-std::string strip_dollar(const std::string& s) { return !s.empty() && s[0] == '$' ? s.substr(1) : s; }
 
 struct Shader {
 	uint32_t kind;
@@ -204,32 +210,27 @@ struct Object {
 struct Instance {
 	std::string data;
 	std::vector<float> transforms;  // 16 per motion sample
-	bool has_shader = false;
-	std::string shader;  // resolved when the scene is flattened, as the reference binds it
+	const Shader* shader = nullptr;  // bound when the instance is read
 };
 
 struct Asm {
 	const Asm* parent = nullptr;
-	std::vector<std::pair<std::string, Shader>> shaders;
+	std::deque<std::pair<std::string, Shader>> shaders;  // (stable addresses)
 	std::vector<std::pair<std::string, Object>> objects;
 	std::vector<std::pair<std::string, std::unique_ptr<Asm>>> subs;
 	std::vector<Instance> instances;
 
-	template <typename T>
-	static T* find(std::vector<std::pair<std::string, T>>& v, const std::string& name) {
-		for (auto& e : v)
-			if (e.first == name) return &e.second;
-		return nullptr;
+	// the first definition of the name
+	template <typename V>
+	static int find(const V& v, const std::string& name) {
+		for (size_t i = 0; i < v.size(); ++i)
+			if (v[i].first == name) return (int)i;
+		return -1;
 	}
-	// a later definition of a name replaces the earlier one in its place
-	template <typename T>
-	static T& put(std::vector<std::pair<std::string, T>>& v, const std::string& name, T value) {
-		if (T* e = find(v, name)) {
-			*e = std::move(value);
-			return *e;
-		}
+	// every definition is kept; lookups find the first
+	template <typename V, typename T>
+	static void put(V& v, const std::string& name, T value) {
 		v.emplace_back(name, std::move(value));
-		return v.back().second;
 	}
 	// scene/assembly.hpp:113-121: the shader of that name here or in an
 	// enclosing assembly
@@ -246,7 +247,7 @@ std::unique_ptr<Asm> parse_assembly(const Node& node, const Asm* parent) {
 	a->parent = parent;
 	for (const Node& ch : node.children) {
 		const std::string& t = ch.type;
-		const std::string name = strip_dollar(ch.name);
+		const std::string& name = ch.name;
 		if (t == "Assembly") {
 			std::unique_ptr<Asm> sub = parse_assembly(ch, a.get());
 			Asm::put(a->subs, name, std::move(sub));
@@ -343,14 +344,11 @@ std::unique_ptr<Asm> parse_assembly(const Node& node, const Asm* parent) {
 				} else if (c.type == "Data") {
 					in.data = c.leaf;
 				} else if (c.type == "SurfaceShaderBind") {
-					in.shader = strip_dollar(c.leaf);
-					in.has_shader = true;
+					in.shader = a->find_shader(c.leaf);
+					if (!in.shader) throw ParseError{"instance binds unknown shader '" + c.leaf + "'"};
 				}
 			}
-			in.data = strip_dollar(in.data);
-			if (in.has_shader && !a->find_shader(in.shader))
-				throw ParseError{"instance binds unknown shader '" + in.shader + "'"};
-			if (!Asm::find(a->objects, in.data) && !Asm::find(a->subs, in.data))
+			if (Asm::find(a->objects, in.data) < 0 && Asm::find(a->subs, in.data) < 0)
 				throw ParseError{"instance of unknown data '" + in.data + "'"};
 			a->instances.push_back(std::move(in));
 		} else if (t == "SubdivisionSurface") {
@@ -486,21 +484,16 @@ void flatten(SceneRead& s, psy_file_scene* f) {
 		st.instances.resize(a->instances.size() ? a->instances.size() : 1);
 		for (size_t i = 0; i < a->instances.size(); ++i) {
 			const Instance& in = a->instances[i];
-			uint32_t kind = PSY_INSTANCE_OBJECT, didx = 0;
-			bool found = false;
-			for (size_t k = 0; k < a->objects.size() && !found; ++k)
-				if (a->objects[k].first == in.data) {
-					didx = (uint32_t)k;
-					found = true;
-				}
-			for (size_t k = 0; k < a->subs.size() && !found; ++k)
-				if (a->subs[k].first == in.data) {
-					kind = PSY_INSTANCE_ASSEMBLY;
-					didx = (uint32_t)k;
-					found = true;
-				}
-			const int32_t sh = in.has_shader ? shader_id(a->find_shader(in.shader)) : -1;
-			st.instances[i] = psy_instance_desc{kind, didx, (uint32_t)(st.transforms.size() / 16),
+			// the object of that name first, as create_object_instance /
+			// create_assembly_instance are tried in the reference
+			uint32_t kind = PSY_INSTANCE_OBJECT;
+			int didx = Asm::find(a->objects, in.data);
+			if (didx < 0) {
+				kind = PSY_INSTANCE_ASSEMBLY;
+				didx = Asm::find(a->subs, in.data);
+			}
+			const int32_t sh = shader_id(in.shader);
+			st.instances[i] = psy_instance_desc{kind, (uint32_t)didx, (uint32_t)(st.transforms.size() / 16),
 			                                    (uint32_t)(in.transforms.size() / 16), sh};
 			st.transforms.insert(st.transforms.end(), in.transforms.begin(), in.transforms.end());
 		}

@@ -176,9 +176,9 @@ Scene $s { RenderSettings { Resolution [4 3] SamplesPerPixel [2] Seed [9] Dicing
     BilinearPatch $p { Vertices [0 0 0  1 0 0  0 1 0  1 1 0.5] }
     Assembly $sub {
       Sphere $inner { Radius [0.2] }
-      Instance { Data [$inner] SurfaceShaderBind [$g] }
       SurfaceShader $g { Type [Emit] Color [9 9 9] }
-      Instance { Data [$inner] SurfaceShaderBind [$g] Transform [1 0 0 0 0 1 0 0 0 0 1 0 3 0 0 1] }
+      Instance { Data [$inner] SurfaceShaderBind [$g] }
+      Instance { Data [$inner] SurfaceShaderBind [$m\ x] Transform [1 0 0 0 0 1 0 0 0 0 1 0 3 0 0 1] }
     }
     Instance { Data [$b] SurfaceShaderBind [$m\ x] }
     Instance { Data [$c] SurfaceShaderBind [$g] Transform [1 0 0 0 0 1 0 0 0 0 1 0 0 0 1 1]
@@ -193,9 +193,10 @@ Scene $s { RenderSettings { Resolution [4 3] SamplesPerPixel [2] Seed [9] Dicing
 
 def test_library_reader_hand_written_file():
     """Comments, escaped names, float forms ("50.", "-1.25"), partial
-    colours and matrices filled from the defaults, shaders found through the
-    enclosing assembly and redefined within one, motion transforms, every
-    object kind, a nested assembly."""
+    colours and matrices filled from the defaults, a shader of the nested
+    assembly's own hiding the enclosing one's and one found in the
+    enclosing assembly, motion transforms, every object kind, a nested
+    assembly."""
     from psychopath_cpp_b200 import api
     sc = S.parse_psy(HAND_WRITTEN)
     mine = api.PsyFile(HAND_WRITTEN)
@@ -208,9 +209,9 @@ def test_library_reader_hand_written_file():
     assert d["cam_transforms"][16:] == [2.0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1]
     assert d["background"] == pytest.approx([0.1, 0.2, 0.0])
     assert len(d["assemblies"]) == 2 and d["assemblies"][0]["children"] == [1]
-    # the nested assembly binds its own later $g (Emit) in both instances
-    sub_shaders = {d["assemblies"][1]["instances"][i][4] for i in range(2)}
-    assert len(sub_shaders) == 1 and d["shaders"][sub_shaders.pop()][0] == 1
+    # the nested assembly's $g is its own Emit shader; $m x the root's
+    sub = d["assemblies"][1]["instances"]
+    assert d["shaders"][sub[0][4]][0] == 1 and d["shaders"][sub[1][4]][0] == 0
 
 
 @pytest.mark.parametrize("bad", [
@@ -256,3 +257,39 @@ def test_library_reader_frames():
     with pytest.raises(_abi.PsyError) as e:
         api.PsyFile(txt, 2)
     assert e.value.code == _abi.PSY_ERR_NO_SCENE
+
+
+def test_library_reader_binds_names_as_the_reference():
+    """Name rules of the reference's Assembly and parser (scene/assembly.hpp:
+    104-157, parser/parser.cpp:298-323): a repeated name keeps every
+    definition and finds the first; an instance binds the shader of that
+    name defined so far (here the enclosing assembly's, as the nested one's
+    comes later); names match as written."""
+    from psychopath_cpp_b200 import _abi, api
+    txt = r"""
+    Scene $s { Assembly {
+      SurfaceShader $g { Type [Lambert] Color [0.1 0.2 0.3] }
+      SurfaceShader $g { Type [Lambert] Color [0.9 0.9 0.9] }
+      Sphere $a { Radius [1] }
+      Sphere $a { Radius [2] }
+      SphereLight $l { Location [0 0 4] Radius [0.5] Color [3 3 3] }
+      Assembly $sub {
+        Sphere $b { Radius [0.5] }
+        Instance { Data [$b] SurfaceShaderBind [$g] }
+        SurfaceShader $g { Type [Emit] Color [7 7 7] }
+        Instance { Data [$b] SurfaceShaderBind [$g] }
+      }
+      Instance { Data [$a] SurfaceShaderBind [$g] }
+      Instance { Data [$l] }
+      Instance { Data [$sub] }
+    } }"""
+    d = _desc_dict(api.PsyFile(txt).desc)
+    root, sub = d["assemblies"]
+    assert len(root["objects"]) == 3 and root["instances"][0][1] == 0       # the first $a
+    assert np.uint32(root["objects"][0][4][3]).view(np.float32) == 1.0
+    first_g = d["shaders"][root["instances"][0][4]]
+    assert first_g[0] == 0 and first_g[1] == pytest.approx([0.1, 0.2, 0.3])  # the first $g
+    assert sub["instances"][0][4] == root["instances"][0][4]                # the root's $g, read so far
+    assert d["shaders"][sub["instances"][1][4]][0] == 1                     # then the nested Emit $g
+    with pytest.raises(_abi.PsyError):
+        api.PsyFile("Scene $s { Assembly { Sphere $a { Radius [1] } Instance { Data [a] } } }")
