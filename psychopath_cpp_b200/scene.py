@@ -456,9 +456,15 @@ def _color(s: str, default=(0.0, 0.0, 0.0)) -> np.ndarray:
 
 
 def _parse_assembly(node: _Node, parent: Optional[Assembly]) -> Assembly:
+    """An Assembly node.  A repeated name keeps its first definition, as
+    the reference's name maps do (scene/assembly.hpp:104-157)."""
     asm = Assembly(parent=parent)
     for ch in node.children:
         t = ch.type
+        key = ch.name[1:]
+        if ((t in ("BilinearPatch", "BicubicPatch", "Sphere", "SphereLight", "RectangleLight") and key in asm.objects)
+                or (t == "SurfaceShader" and key in asm.shaders) or (t == "Assembly" and key in asm.assemblies)):
+            continue
         if t == "Assembly":
             asm.add_assembly(ch.name[1:], _parse_assembly(ch, asm))
         elif t == "BilinearPatch":

@@ -187,3 +187,43 @@ def test_closed_form_partition_is_the_two_ended_loop():
     for v, th in cases:
         pred = lambda x, th=th: x[0] < th
         assert _two_ended_partition(v, pred) == _closed_form_partition(v, pred), (v, th)
+
+
+def test_library_reader_matches_reference_parser(ref_available, tmp_path):
+    """The library's .psy reader (psy_file_parse) against the reference's
+    own parser (Parser::parse_next_frame, in oracle/_ref) on the same files:
+    the same BVH4 records and light trees in every assembly, for generated
+    scenes, the hand-written file and a file that repeats a light's name
+    with another power (the reference finds the first definition)."""
+    from oracle import psyref
+    from tests.test_scene_format import HAND_WRITTEN
+    repeated = r"""
+    Scene $s { RenderSettings { Resolution [8 6] SamplesPerPixel [1] }
+      Camera { Fov [40] Transform [1 0 0 0 0 1 0 0 0 0 1 0 0 0 -5 1] }
+      Assembly {
+        SurfaceShader $m { Type [Lambert] Color [0.5 0.5 0.5] }
+        SphereLight $l { Location [0 0 4] Radius [0.5] Color [3 3 3] }
+        SphereLight $l { Location [1 0 4] Radius [0.5] Color [30 30 30] }
+        SphereLight $k { Location [2 0 4] Radius [0.25] Color [5 5 5] }
+        Sphere $a { Radius [1] }
+        Instance { Data [$a] SurfaceShaderBind [$m] }
+        Instance { Data [$l] }
+        Instance { Data [$k] }
+      }
+    }"""
+    texts = [HAND_WRITTEN, repeated,
+             scenes.many_light_scene(9, res=(32, 18), spp=1, n_patches=30, n_groups=15, n_lights=250).to_psy(),
+             scenes.motion_patch_scene(1, n=3).to_psy(),
+             scenes.rect_light_scene(1, res=(8, 6), spp=1, n_spheres=3).to_psy()]
+    for i, txt in enumerate(texts):
+        path = tmp_path / ("s%d.psy" % i)
+        path.write_text(txt)
+        ref = psyref.RefScene(psy_path=str(path))
+        mine = api.PsyFile(txt)
+        for a in range(ref.assembly_count()):
+            _compare_bvh4(ref.bvh4_nodes(a), api.build_bvh4_records(mine, a), True)
+            lt = ref.light_tree(a)
+            ml = api.build_light_tree(mine, a)
+            np.testing.assert_array_equal(lt["meta"], ml["meta"])
+            np.testing.assert_array_equal(lt["energy"], ml["energy"])
+            np.testing.assert_array_equal(lt["bounds"], ml["bounds"])
