@@ -201,7 +201,8 @@ int psy_build_light_tree(const psy_scene_desc* scene, uint32_t assembly, uint64_
  */
 typedef struct psy_file_scene psy_file_scene;
 typedef struct psy_render_settings {
-	uint32_t width, height, spp, seed;  /* RenderSettings: Resolution, SamplesPerPixel, Seed */
+	uint32_t width, height, spp, seed;  /* RenderSettings: Resolution, SamplesPerPixel, Seed (default 1 each) */
+	const char* output_path;            /* Output: Path ("" when none), owned by the psy_file_scene */
 } psy_render_settings;
 int psy_file_parse(const char* text, size_t len, uint32_t frame, psy_file_scene** out, char* err, size_t err_len);
 const psy_scene_desc* psy_file_scene_desc(const psy_file_scene* scene);

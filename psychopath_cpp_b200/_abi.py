@@ -87,7 +87,8 @@ class SceneStats(C.Structure):
 
 
 class RenderSettings(C.Structure):
-    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("seed", C.c_uint32)]
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("seed", C.c_uint32),
+                ("output_path", C.c_char_p)]
 
 
 class RaySoA(C.Structure):

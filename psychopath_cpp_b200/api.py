@@ -162,7 +162,8 @@ class PsyFile:
         self.h = h
         s = _abi.RenderSettings()
         self.L.psy_file_render_settings(h, C.byref(s))
-        self.settings = {k: int(getattr(s, k)) for k, _ in _abi.RenderSettings._fields_}
+        self.settings = {k: int(getattr(s, k)) for k in ("width", "height", "spp", "seed")}
+        self.output_path = (s.output_path or b"").decode()
 
     @classmethod
     def read(cls, path: str, frame: int = 0) -> "PsyFile":

@@ -374,7 +374,8 @@ struct psy_file_scene {
 	std::vector<psy_shader_desc> shaders;
 	std::vector<float> cam_transforms, cam_fovs, cam_apertures, cam_focus;
 	psy_scene_desc desc{};
-	psy_render_settings settings{64, 64, 1, 1};
+	psy_render_settings settings{1, 1, 1, 1, ""};
+	std::string output_path;
 };
 
 namespace {
@@ -386,7 +387,8 @@ struct SceneRead {
 	float background[3] = {0, 0, 0};
 	bool has_dice_rate = false;
 	float dice_rate = 0.25f;
-	psy_render_settings settings{64, 64, 1, 1};
+	psy_render_settings settings{1, 1, 1, 1, ""};  // parser/parser.cpp:61-64
+	std::string output_path;
 };
 
 struct NoFrame {};
@@ -405,7 +407,18 @@ SceneRead read_scene(const Node& tree, uint32_t frame) {
 	if (!sn) throw NoFrame{};
 	SceneRead s;
 	for (const Node& node : sn->children) {
-		if (node.type == "RenderSettings") {
+		if (node.type == "Output") {
+			// Path: the text from the first to the last double quote, the
+			// quotes taken out (parser/parser.cpp:66-76)
+			for (const Node& c : node.children) {
+				if (c.type != "Path") continue;
+				const size_t a = c.leaf.find('"'), b = c.leaf.rfind('"');
+				if (a == std::string::npos || b == a) continue;
+				s.output_path.clear();
+				for (size_t i = a; i <= b; ++i)
+					if (c.leaf[i] != '"') s.output_path += c.leaf[i];
+			}
+		} else if (node.type == "RenderSettings") {
 			for (const Node& c : node.children) {
 				if (c.type == "Resolution") {
 					const std::vector<long> v = ints(c.leaf);
@@ -543,6 +556,8 @@ void flatten(SceneRead& s, psy_file_scene* f) {
 	d.shader_count = (uint32_t)shader_list.size();
 	d.shaders = f->shaders.data();
 	f->settings = s.settings;
+	f->output_path = s.output_path;
+	f->settings.output_path = f->output_path.c_str();
 	f->scene = std::shared_ptr<void>(s.root.release(), [](void* p) { delete static_cast<Asm*>(p); });
 }
 

@@ -293,3 +293,14 @@ def test_library_reader_binds_names_as_the_reference():
     assert d["shaders"][sub["instances"][1][4]][0] == 1                     # then the nested Emit $g
     with pytest.raises(_abi.PsyError):
         api.PsyFile("Scene $s { Assembly { Sphere $a { Radius [1] } Instance { Data [a] } } }")
+
+
+def test_library_reader_output_path_and_defaults():
+    """Output Path as the reference takes it (the text between the first
+    and last double quote, quotes removed) and its render-setting defaults
+    (parser/parser.cpp:61-76): 1 x 1 pixels, 1 sample, seed 1."""
+    from psychopath_cpp_b200 import api
+    f = api.PsyFile('Scene $s { Output { Path ["out/a"b".png"] } Assembly { } }')
+    assert f.output_path == "out/ab.png"
+    assert f.settings == {"width": 1, "height": 1, "spp": 1, "seed": 1}
+    assert api.PsyFile("Scene $s { Assembly { } }").output_path == ""
