@@ -103,7 +103,7 @@ def flatten(scene: Scene):
                 kind, didx = _abi.PSY_INSTANCE_ASSEMBLY, sub_pos[inst.data]
             else:
                 raise KeyError("instance of unknown data %r" % inst.data)
-            sh = a.find_shader(inst.shader) if inst.shader is not None else None
+            sh = a.shader_of(inst)
             insts[ii] = _abi.InstanceDesc(kind, didx, len(xforms), len(inst.transforms), shader_id(sh))
             xforms.extend(inst.transforms)
         xf = np.ascontiguousarray(np.array(xforms, dtype=F32).reshape(-1)) if xforms else np.zeros(16, F32)
@@ -591,7 +591,7 @@ def flat_indices(scene: Scene) -> Tuple[Dict[int, int], Dict[Tuple[int, str], in
         for name in a.objects:
             objects[(ai, name)] = len(objects)
         for inst in a.instances:
-            sh = a.find_shader(inst.shader) if inst.shader is not None else None
+            sh = a.shader_of(inst)
             if sh is not None and id(sh) not in shaders:
                 shaders[id(sh)] = len(shaders)
     return shaders, objects, len(shaders), len(objects)

@@ -149,6 +149,10 @@ class Instance:
     data: str
     transforms: List[np.ndarray] = field(default_factory=list)
     shader: Optional[str] = None
+    # the shader bound when the instance was read from a file: the one of
+    # that name defined so far, as the reference binds it
+    # (parser/parser.cpp:298-323); None: looked up by name when flattened
+    bound: Optional["SurfaceShader"] = field(default=None, repr=False, compare=False)
 
     def __post_init__(self):
         self.transforms = [_f32(t).reshape(4, 4) for t in self.transforms]
@@ -181,6 +185,12 @@ class Assembly:
         inst = Instance(data, list(transforms), shader)
         self.instances.append(inst)
         return inst
+
+    def shader_of(self, inst: "Instance") -> Optional[SurfaceShader]:
+        """The shader an instance of this assembly renders with."""
+        if inst.bound is not None:
+            return inst.bound
+        return self.find_shader(inst.shader) if inst.shader is not None else None
 
     def find_shader(self, name: str) -> Optional[SurfaceShader]:
         """Shader lookup through the parent chain
@@ -537,7 +547,7 @@ def _parse_assembly(node: _Node, parent: Optional[Assembly]) -> Assembly:
                     raise PsyParseError("instance binds unknown shader %r" % shader)
             if data not in asm.objects and data not in asm.assemblies:
                 raise PsyParseError("instance of unknown data %r" % data)
-            asm.add_instance(data, xf, shader)
+            asm.add_instance(data, xf, shader).bound = asm.find_shader(shader) if shader is not None else None
         elif t in ("RectangleLight", "SubdivisionSurface"):
             raise PsyParseError("%s is outside the supported hot path" % t)
     return asm

@@ -293,6 +293,13 @@ def test_library_reader_binds_names_as_the_reference():
     assert d["shaders"][sub["instances"][1][4]][0] == 1                     # then the nested Emit $g
     with pytest.raises(_abi.PsyError):
         api.PsyFile("Scene $s { Assembly { Sphere $a { Radius [1] } Instance { Data [a] } } }")
+    # the Python reader binds and resolves names the same way
+    sc = S.parse_psy(txt)
+    py_desc, keep = api.flatten(sc)
+    pd = _desc_dict(py_desc)
+    assert [i[4] for i in pd["assemblies"][1]["instances"]] == [i[4] for i in sub["instances"]]
+    assert [pd["shaders"][i[4]] for i in pd["assemblies"][1]["instances"]] == \
+        [d["shaders"][i[4]] for i in sub["instances"]]
 
 
 def test_library_reader_output_path_and_defaults():
